@@ -1,0 +1,371 @@
+"""Benchmark of the SBR hot path on B200: angle-frequency samples/s and Mray-bounces/s.
+
+Workload (default, one GPU): square trihedral corner reflector, 1 m edges, 3 x
+100x100x2 = 60,000 triangles, 10 GHz, 10 rays/lambda over the bounding aperture
+(G = sqrt(3) m, 578 x 578 = 334,084 rays per angle), max 3 bounces, 2-D sweep
+theta = 0..90 x phi = 0..90 deg at 1 deg (8,281 angles), all drained by one
+persistent launch.  Synthetic, seeded mesh (no dataset is involved).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`value`      whole-job samples/s with the plan resident in HBM (sbr_plan_execute on
+             torch's current stream, CUDA events, L2 flushed between steps).
+`e2e`        the same metric through sbr_run with host arrays in and out (frames,
+             item table H2D, fields D2H inside the timed region).
+`roofline`   dominant kernel (k_trace): algorithmic FP32 work per closest-hit
+             query on the reference SAH tree, 27 V_box + 57 V_tri FLOP, with
+             V_box / V_tri counted by the instrumented CPU oracle on a sample of the
+             same sweep; peak = FP32 SGEMM throughput measured here (the driver's
+             peak file has HBM and bf16 only).
+`cpu_baseline` the reference's own per-ray routine (src/cuda/rtKernels.cu) compiled
+             for the host (oracle/_ref), OpenMP over all host cores, timed on a
+             bounded sample of the same sweep.
+Under torchrun (N > 1) every rank sweeps its own angle set (phi offset by
+rank * 0.1 deg): weak scaling, no collective on the data path; the time is the
+max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+C0 = 299792458.0
+FLOP_PER_BOX = 27
+FLOP_PER_TRI = 57
+
+
+def workload(rank: int = 0):
+    from sagittasbr_b200 import meshes as M
+    v, t = M.trihedral(1.0, 100)
+    G = 2.0 * M.bounding_radius(v)
+    n = M.rays_for(1e10, G)
+    th, ph = np.meshgrid(np.arange(0.0, 91.0), np.arange(0.0, 91.0), indexing="ij")
+    th = th.ravel()
+    ph = ph.ravel() + 0.1 * rank
+    return dict(verts=v, tris=t, theta=th, phi=ph, freqs=[1e10], nx=n, ny=n, G=G, max_bounces=3, R=1.0,
+                name=f"trihedral_60k_10GHz_{n}x{n}_3b_{th.size}ang")
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+                for nm, val in zip(names, r[5:9]):
+                    if val.strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def fp32_peak_tflops(torch) -> float:
+    """Dense FP32 (no TF32) SGEMM throughput, best of 5 at 8192^3."""
+    torch.backends.cuda.matmul.allow_tf32 = False
+    n = 8192
+    a = torch.randn(n, n, device="cuda")
+    b = torch.randn(n, n, device="cuda")
+    for _ in range(2):
+        a @ b
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        a @ b
+        e.record()
+        e.synchronize()
+        best = max(best, 2 * n ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    del a, b
+    return best
+
+
+def cpu_reference(w, budget_s: float, threads: int = 0, want_counts: bool = True):
+    """The reference's own per-ray code (oracle/_ref) on a bounded sample of the
+    sweep; returns (samples/s, bounces/s, sample description, V_box, V_tri)."""
+    from oracle import oracle as O
+    kind = "32fast" if O.ref_available("32fast") else None
+    idx = np.random.default_rng(7).permutation(w["theta"].size)
+    done, bounces, t_used = 0, 0, 0.0
+    while t_used < budget_s and done < idx.size:
+        sel = idx[done:done + 4]
+        t0 = time.perf_counter()
+        if kind:
+            out = O.ref_sweep(w["verts"], w["tris"], w["theta"][sel], w["phi"][sel], w["freqs"], w["nx"], w["ny"],
+                              w["G"], w["max_bounces"], w["R"], kind=kind, threads=threads)
+        else:
+            out = O.sweep(w["verts"], w["tris"], w["theta"][sel], w["phi"][sel], w["freqs"], w["nx"], w["ny"],
+                          w["G"], w["max_bounces"], w["R"], precision=32, threads=threads)
+        t_used += time.perf_counter() - t0
+        bounces += int(out.counts["bounces"].sum())
+        done += sel.size
+    vbox = vtri = None
+    if want_counts:
+        sel = idx[:2]
+        o = O.sweep(w["verts"], w["tris"], w["theta"][sel], w["phi"][sel], w["freqs"], w["nx"], w["ny"], w["G"],
+                    w["max_bounces"], w["R"], precision=64, accel="tree", threads=threads)
+        q = o.counts["queries"].sum()
+        vbox, vtri = float(o.counts["box_tests"].sum() / q), float(o.counts["tri_tests"].sum() / q)
+    sample = (f"{done} of {w['theta'].size} angles (random, seed 7) at full {w['nx']}x{w['ny']} rays, "
+              f"{'reference rtKernels.cu host build (oracle/_ref, FP32, -O3)' if kind else 'FP32 oracle port'}")
+    return done / t_used, bounces / t_used, sample, vbox, vtri, ("reference" if kind else "port")
+
+
+def read_traffic():
+    """DRAM bytes per k_trace launch from the committed ncu summary (or None)."""
+    p = os.path.join(ROOT, "profiles", "k_trace_trihedral.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("dram_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def run_reference_arm(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    w = workload(0)
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        pass
+    per_step = []
+    bps = []
+    sample = ""
+    kind = "port"
+    budget = max(2.0, 60.0 / max(1, args.steps + args.warmup))
+    for s in range(args.warmup + args.steps):
+        sps, bounces, sample, _, _, kind = cpu_reference(w, budget, threads, want_counts=False)
+        if s >= args.warmup:
+            per_step.append(sps)
+            bps.append(bounces)
+    v = float(np.mean(per_step))
+    line = {
+        "impl": "reference", "metric": "angle-freq samples/s", "value": v, "unit": "samples/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * w["theta"].size / v, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded trihedral mesh)",
+        "config": {"workload": w["name"], "angles": int(w["theta"].size), "rays_per_angle": w["nx"] * w["ny"],
+                   "max_bounces": w["max_bounces"], "sampled": True},
+        "mray_bounces_per_s": float(np.mean(bps)) / 1e6,
+        "cpu_baseline": {"value": v, "unit": "samples/s", "cores": threads, "kind": kind, "sample": sample},
+        "e2e": {"value": v, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--per-angle-stride", type=int, default=8,
+                    help="per-angle mode is timed on every n-th angle of the sweep")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+    import sagittasbr_b200 as sbr
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    w = workload(rank)
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    scene = sbr.Scene(w["verts"], w["tris"], device=local)
+    job = sbr.JobSpec(w["theta"], w["phi"], w["freqs"], w["nx"], w["ny"], w["G"], w["max_bounces"], w["R"])
+    plan = sbr.Plan(scene, [job], mode=sbr.MODE_BATCHED, precision=sbr.PREC_MIXED, stream=sp)
+    info = plan.info
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        plan.execute()
+    res = plan.results()
+    bounces_step, queries_step = res.bounces, res.queries
+    barrier()
+    clocks = Clocks(local) if rank == 0 else None
+    per = []
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for _ in range(args.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        plan.execute()
+        e1.record(stream)
+        per.append((e0, e1))
+    t_end.record(stream)
+    barrier()
+    clk = clocks.stop() if clocks else None
+    total_ms = t_start.elapsed_time(t_end)
+    kern_ms = float(np.mean([a.elapsed_time(b) for a, b in per]))
+    ms = torch.tensor([total_ms / args.steps, kern_ms], device="cuda", dtype=torch.float64)
+    if dist is not None:
+        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    step_ms, kern_ms = float(ms[0]), float(ms[1])
+    samples = info["n_samples"]
+    value = samples * ws / (step_ms * 1e-3)
+
+    # end to end through sbr_run (host arrays in, host arrays out)
+    e2e_ms = []
+    for s in range(1 + min(args.steps, 3)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r2 = sbr.run(scene, job, mode=sbr.MODE_BATCHED, precision=sbr.PREC_MIXED)
+        if s:
+            e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_t = torch.tensor([float(np.mean(e2e_ms))], device="cuda", dtype=torch.float64)
+    if dist is not None:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_value = samples * ws / (float(e2e_t[0]) * 1e-3)
+    assert np.array_equal(r2.field, res.field), "sbr_run and plan results differ"
+
+    # per-angle mode (the reference's loop structure) on a subset of the same sweep
+    sub = slice(0, None, args.per_angle_stride)
+    pjob = sbr.JobSpec(w["theta"][sub], w["phi"][sub], w["freqs"], w["nx"], w["ny"], w["G"], w["max_bounces"], w["R"])
+    pplan = sbr.Plan(scene, [pjob], mode=sbr.MODE_PER_ANGLE, precision=sbr.PREC_FP32, stream=sp)
+    pplan.execute()
+    torch.cuda.synchronize()
+    pa0, pa1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    pa0.record(stream)
+    pplan.execute()
+    pa1.record(stream)
+    torch.cuda.synchronize()
+    pa_ms = pa0.elapsed_time(pa1)
+    per_angle_value = pplan.info["n_samples"] / (pa_ms * 1e-3)
+    pres = pplan.results()
+    bplan = sbr.Plan(scene, [pjob], mode=sbr.MODE_BATCHED, precision=sbr.PREC_MIXED, stream=sp)
+    bplan.execute()
+    bres = bplan.results()
+    with np.errstate(divide="ignore"):
+        d_db = np.abs(pres.rcs_dbsm - bres.rcs_dbsm)
+
+    if dist is not None:
+        dist.barrier()
+    if rank != 0:
+        plan.close()
+        scene.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
+
+    peak = fp32_peak_tflops(torch)
+    cpu = None
+    vbox = vtri = None
+    if not args.no_cpu and ws == 1:
+        sps, bps, sample, vbox, vtri, kind = cpu_reference(w, 15.0)
+        cpu = {"value": sps, "unit": "samples/s", "cores": os.cpu_count(), "kind": kind, "sample": sample,
+               "mray_bounces_per_s": bps / 1e6}
+    roof = None
+    if vbox is not None:
+        flop_q = FLOP_PER_BOX * vbox + FLOP_PER_TRI * vtri
+        achieved = queries_step * flop_q / (kern_ms * 1e-3) / 1e12
+        traffic = read_traffic()
+        roof = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": traffic, "kernel": "k_trace (persistent) + k_finalize",
+                "flop_per_query": flop_q, "v_box": vbox, "v_tri": vtri, "queries_per_launch": queries_step,
+                "peak_source": "FP32 SGEMM 8192^3 measured in this run (no FP32 figure in MEASURED_PEAKS.json)",
+                "hbm_view": {"bytes_per_query": 48 * (vbox + vtri),
+                             "achieved_GBs": queries_step * 48 * (vbox + vtri) / (kern_ms * 1e-3) / 1e9,
+                             "note": "reference-tree node+triangle bytes; served from L1/L2, not HBM"}}
+    line = {
+        "metric": "angle-freq samples/s", "value": value, "unit": "samples/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32 traversal + fp64 phase/sums",
+        "data": "synthetic (seeded trihedral mesh)",
+        "config": {"workload": w["name"], "angles": int(w["theta"].size), "freqs": len(w["freqs"]),
+                   "rays_per_angle": w["nx"] * w["ny"], "rays_launched_per_step": info["n_rays_clipped"],
+                   "max_bounces": w["max_bounces"], "mode": "batched persistent", "precision": "mixed",
+                   "l2": "flushed before every step (256 MiB write inside the timed region)",
+                   "parallelism": f"{ws} GPU(s), independent sweeps"},
+        "mray_bounces_per_s": bounces_step * ws / (step_ms * 1e-3) / 1e6,
+        "closest_hit_queries_per_s": queries_step * ws / (step_ms * 1e-3),
+        "kernel_ms": kern_ms,
+        "per_angle": {"value": per_angle_value, "unit": "samples/s", "precision": "fp32 (reference arithmetic)",
+                      "angles": pplan.info["n_samples"], "ms": pa_ms, "launches": pplan.info["launches_per_execute"],
+                      "max_abs_ddb_vs_batched": float(np.nanmax(d_db)),
+                      "batched_speedup": value / ws / per_angle_value},
+        "e2e": {"value": e2e_value, "unit": "samples/s", "h2d_bytes_per_step": info["h2d_bytes"],
+                "d2h_bytes_per_step": info["d2h_bytes"], "ms_per_step": float(e2e_t[0])},
+        "gpu_launches": int(info["launches_per_execute"]) * args.steps,
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+    plan.close()
+    scene.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

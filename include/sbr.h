@@ -1,0 +1,231 @@
+/* sbr.h -- C ABI of libsbr, the B200-native shooting-and-bouncing-rays (SBR)
+ * monostatic RCS engine.
+ *
+ * This boundary replaces SagittaSBR's device seam
+ *
+ *     sweepResults runSweep(const simulationConfig&, deviceBuffers&,
+ *                           const bvhGpuData&, std::ostream&)      include/sim/sweep.hpp:15-16
+ *
+ * and the set-up that feeds it in runRcsApp (src/app/rtRcsEntry.cu:115-196:
+ * de-indexing, model scale, buildBvh, cudaMalloc/cudaMemcpy of triangles and
+ * nodes, allocateDeviceBuffers).  Plain pointers and sizes only; every call
+ * returns a status (the reference calls cudaDeviceReset + exit(1) on any CUDA
+ * error, src/cuda/cudaUtils.cu:6-14; this library never exits).
+ *
+ * Threading: a scene or plan handle is used by one host thread at a time.
+ * Device memory belongs to the scene / plan that allocated it.
+ */
+#ifndef SBR_H
+#define SBR_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SBR_ABI_VERSION 1
+
+/* ------------------------------------------------------------------ status */
+typedef int32_t sbr_status;
+#define SBR_OK 0
+#define SBR_ERR_INVALID_ARG 1   /* null pointer, bad size, bad enum           */
+#define SBR_ERR_EMPTY_MESH 2    /* no triangles (rtRcsEntry.cu:109-113)       */
+#define SBR_ERR_BAD_INDEX 3     /* vertex index out of range (:126-130)       */
+#define SBR_ERR_NONFINITE 4     /* NaN/Inf vertex or parameter                */
+#define SBR_ERR_TOO_LARGE 5     /* grid or mesh beyond the supported size     */
+#define SBR_ERR_CUDA 6          /* CUDA runtime error (message in last_error) */
+#define SBR_ERR_OOM 7           /* device allocation failed                   */
+#define SBR_ERR_NO_DEVICE 8     /* no usable sm_100 device                    */
+#define SBR_ERR_STACK 9         /* traversal stack overflow reported by GPU   */
+#define SBR_ERR_TIMEOUT 10      /* iteration budget exceeded on the GPU       */
+#define SBR_ERR_CANCELLED 11    /* sbr_scene_cancel() observed by the kernel  */
+#define SBR_ERR_IO 12           /* file could not be read / written           */
+#define SBR_ERR_PARSE 13        /* malformed model / config file             */
+#define SBR_ERR_UNSUPPORTED 14  /* option not available in this build         */
+
+/* Short name of a status code (static string). */
+const char* sbr_status_str(sbr_status s);
+/* Detail message of the last failing call on this host thread (static per thread). */
+const char* sbr_last_error(void);
+int32_t sbr_abi_version(void);
+
+/* ------------------------------------------------------------------- scene */
+typedef struct sbr_scene sbr_scene;
+
+typedef struct sbr_build_opts {
+    double model_scale;   /* vertices are multiplied by this (--model-scale, rtRcsEntry.cu:137-145); 0 -> 1 */
+    int32_t device;       /* CUDA device ordinal; -1 -> current device */
+    int32_t leaf_size;    /* max triangles per BVH leaf; 0 -> 4 (bvhBuilder.hpp:14) */
+    int32_t bin_count;    /* SAH bins; 0 -> 16 (bvhBuilder.hpp:15) */
+    int32_t n_threads;    /* host threads for the build; 0 -> all */
+    int32_t want_fp64;    /* also upload FP64 triangles (needed by SBR_PREC_FP64); -1 -> lazily */
+    int32_t reserved[3];
+} sbr_build_opts;
+
+typedef struct sbr_scene_info {
+    int64_t n_triangles;
+    int64_t n_nodes_bin;      /* binary SAH nodes */
+    int64_t n_nodes_gpu;      /* nodes of the traversal layout in HBM */
+    int64_t device_bytes;     /* scene bytes resident on the device */
+    double aabb_lo[3];
+    double aabb_hi[3];
+    double build_ms;          /* host BVH build time */
+    int32_t device;
+    int32_t bvh_depth;
+} sbr_scene_info;
+
+/* Copies the indexed triangle mesh (xyz: nverts*3 floats, tri_idx: ntris*3
+ * indices), builds the BVH on the host and uploads it.  The caller keeps its
+ * buffers.  Replaces rtRcsEntry.cu:115-196. */
+sbr_status sbr_scene_create(const float* xyz, size_t nverts, const uint32_t* tri_idx, size_t ntris,
+                            const sbr_build_opts* opts, sbr_scene** out);
+sbr_status sbr_scene_destroy(sbr_scene* scene);
+sbr_status sbr_scene_info_get(const sbr_scene* scene, sbr_scene_info* out);
+/* Asks running kernels of this scene to stop at their next work item
+ * (they return SBR_ERR_CANCELLED); sbr_scene_reset_cancel clears it. */
+sbr_status sbr_scene_cancel(sbr_scene* scene);
+sbr_status sbr_scene_reset_cancel(sbr_scene* scene);
+
+/* --------------------------------------------------------------------- job */
+/* One job = a list of incidence angles traced on one ray grid, with a set of
+ * frequencies that share that grid.  The reference runs one (angle, frequency)
+ * per iteration with nx*ny rays over a square of side grid_size placed
+ * 10*grid_size from the origin (src/app/sweep.cu:50-55,336-397). */
+typedef struct sbr_job {
+    const double* theta_deg;  /* [n_angles] */
+    const double* phi_deg;    /* [n_angles] */
+    int64_t n_angles;
+    const double* freq_hz;    /* [n_freqs] */
+    int64_t n_freqs;
+    int32_t nx, ny;           /* ray grid (n_x, n_y) */
+    double grid_size;         /* launcher side G in metres (grid_size) */
+    int32_t max_bounces;      /* max_bounces */
+    double reflection_const;  /* reflection_const (R per bounce, 1 = PEC) */
+} sbr_job;
+
+#define SBR_MODE_BATCHED 0    /* one persistent launch drains every (job, angle, tile) item; all
+                                 frequencies of a job come from one trace */
+#define SBR_MODE_PER_ANGLE 1  /* the reference's loop: one trace + PO launch per (angle, frequency) */
+
+#define SBR_PREC_MIXED 0      /* FP32 traversal, FP64 path length / phase reduction / field sums */
+#define SBR_PREC_FP32 1       /* the reference FP32 build's arithmetic (launch plane at 10 G, FP32 phase) */
+#define SBR_PREC_FP64 2       /* everything in FP64 (the reference USE_DOUBLE build's arithmetic) */
+
+#define SBR_POL_SCALAR 0      /* the reference's scalar PO term (HH == VV) */
+#define SBR_POL_HHVV 1        /* PEC E-vector tracking; fields for HH and VV */
+
+typedef struct sbr_run_opts {
+    int32_t mode;             /* SBR_MODE_* */
+    int32_t precision;        /* SBR_PREC_* */
+    int32_t polarization;     /* SBR_POL_* */
+    int32_t use_graph;        /* capture plan execution in a CUDA graph (batched mode) */
+    void* stream;             /* cudaStream_t to launch on; NULL -> the scene's own stream */
+    int32_t ctas_per_sm;      /* persistent grid size per SM; 0 -> occupancy-derived */
+    int32_t reserved[7];
+} sbr_run_opts;
+
+/* Results for every (job, angle, frequency[, polarization]) in job order, then
+ * angle order, then frequency order (then HH, VV).  Each array may be NULL. */
+typedef struct sbr_result {
+    double* field;            /* [n_samples * n_pol * 2]: re, im of the scattered field sum */
+    double* sigma_m2;         /* [n_samples * n_pol]: 4*pi*|field|^2 (sweep.cu:228-230) */
+    double* rcs_dbsm;         /* [n_samples * n_pol]: 10*log10(max(sigma, 1e-10)) (sweep.cu:231) */
+    uint64_t* stats;          /* [n_job_angles * 4]: rays, hit rays, bounces, closest-hit queries */
+    double device_ms;         /* out: device time of the trace + reduce launches */
+} sbr_result;
+
+/* Plans hold the per-angle launcher frames, the work-item table and the device
+ * result buffers; executing a plan touches no host memory. */
+typedef struct sbr_plan sbr_plan;
+
+typedef struct sbr_plan_info {
+    int64_t n_samples;        /* sum over jobs of n_angles * n_freqs */
+    int64_t n_job_angles;     /* sum over jobs of n_angles */
+    int64_t n_items;          /* work items (ray tiles after aperture clipping) */
+    int64_t n_rays_clipped;   /* rays actually launched (inside the projected AABB) */
+    int64_t n_rays_grid;      /* sum of nx*ny over job angles */
+    int32_t n_pol;
+    int32_t launches_per_execute; /* kernels launched by one sbr_plan_execute */
+    int64_t device_bytes;
+    int64_t h2d_bytes;        /* bytes sbr_plan_create copies host -> device */
+    int64_t d2h_bytes;        /* bytes sbr_plan_results copies device -> host (field, stats, error word) */
+} sbr_plan_info;
+
+sbr_status sbr_plan_create(sbr_scene* scene, const sbr_job* jobs, size_t n_jobs, const sbr_run_opts* opts,
+                           sbr_plan** out);
+/* Launches the plan on opts->stream (or the scene stream); asynchronous. */
+sbr_status sbr_plan_execute(sbr_plan* plan);
+/* Waits for the plan and copies results to host arrays (any may be NULL). */
+sbr_status sbr_plan_results(sbr_plan* plan, sbr_result* out);
+/* Device pointers of the plan's result arrays (valid until destroy). */
+sbr_status sbr_plan_device_results(sbr_plan* plan, const double** d_field, const uint64_t** d_stats);
+sbr_status sbr_plan_info_get(const sbr_plan* plan, sbr_plan_info* out);
+sbr_status sbr_plan_destroy(sbr_plan* plan);
+
+/* One call: plan, execute, copy results to host, release.  Host arrays in, host
+ * arrays out.  Replaces runSweep's loop (src/app/sweep.cu:332-441). */
+sbr_status sbr_run(sbr_scene* scene, const sbr_job* jobs, size_t n_jobs, sbr_result* out,
+                   const sbr_run_opts* opts);
+
+/* ------------------------------------------------------------- diagnostics */
+#define SBR_MAX_REC 16
+/* Per-ray record: the reference's hit buffers (include/app/deviceBuffers.hpp:6-15)
+ * plus the triangle ids of the first hits (index in the caller's mesh). */
+typedef struct sbr_ray_record {
+    int32_t count;            /* hitCount */
+    int32_t flags;            /* bit 0: ray launched (inside the clipped aperture) */
+    double dist;              /* hitDist, summed from the reference launcher plane */
+    float normal[3];          /* last hit normal */
+    float lastdir[3];         /* incoming direction at the last hit */
+    int32_t tri[SBR_MAX_REC]; /* hit triangle ids, -1 padded */
+} sbr_ray_record;
+
+/* Traces every ray of every angle of one job and writes nx*ny records per angle
+ * (angle-major, row-major j*nx + i) to the host array `out`. */
+sbr_status sbr_trace_records(sbr_scene* scene, const sbr_job* job, const sbr_run_opts* opts,
+                             sbr_ray_record* out);
+
+/* --------------------------------------------------------- entry surface */
+/* config.txt keys and defaults of include/app/config.hpp:8-25. */
+typedef struct sbr_config {
+    double phi_start, phi_end;
+    int32_t phi_samples;
+    double theta_start, theta_end;
+    int32_t theta_samples;
+    double grid_size;
+    int32_t nx, ny;
+    int32_t tpb_x, tpb_y;     /* parsed, unused (as in the reference) */
+    int32_t max_bounces;
+    double reflection_const;
+    double freq;
+    int32_t show_info_gpu;
+    int32_t show_hit_stats;
+    double model_scale;
+    char model_path[4096];
+    int32_t freq_source;      /* 0 default, 1 config file, 2 command line */
+    /* optional keys of this engine (absent from reference configs, which keep the defaults) */
+    int32_t precision;        /* key "precision": SBR_PREC_* (default SBR_PREC_MIXED) */
+    int32_t mode;             /* key "engine_mode": SBR_MODE_* (default SBR_MODE_BATCHED) */
+} sbr_config;
+
+/* loadConfig (src/app/config.cpp:39-155): reads `default_path` (or --config),
+ * applies --model, --model-scale and the first bare argument as frequency.
+ * Never exits: a missing file keeps defaults; a flag without value returns
+ * SBR_ERR_INVALID_ARG.  Warnings go to stderr as in the reference. */
+sbr_status sbr_config_load(const char* default_path, int argc, const char* const* argv, sbr_config* out);
+/* theta-major angle grid of src/app/sweep.cu:336-347 (n = theta_samples*phi_samples). */
+sbr_status sbr_config_angles(const sbr_config* cfg, double* theta_deg, double* phi_deg);
+/* OBJ reader (v / f records; polygons fan-triangulated).  *xyz and *tri_idx are
+ * allocated with malloc; release with sbr_free. */
+sbr_status sbr_load_obj(const char* path, float** xyz, size_t* nverts, uint32_t** tri_idx, size_t* ntris);
+void sbr_free(void* p);
+/* Writes rcs_results.csv in the reference layout (rtRcsEntry.cu:298-303, sweep.cu:540-544). */
+sbr_status sbr_write_csv(const char* path, const sbr_config* cfg, const double* theta_deg, const double* phi_deg,
+                         const double* sigma_m2, const double* rcs_dbsm, int64_t n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SBR_H */

@@ -1,0 +1,122 @@
+// common.hpp -- internal types shared by the host set-up and the sm_100a kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "sbr.h"
+
+namespace sbr {
+
+// ------------------------------------------------------------------ errors
+// Thread-local detail message behind sbr_last_error().
+void set_error(const std::string& msg);
+sbr_status fail(sbr_status s, const std::string& msg);
+sbr_status cuda_fail(cudaError_t e, const char* what);
+
+#define SBR_CUDA(call)                                      \
+    do {                                                    \
+        cudaError_t e__ = (call);                           \
+        if (e__ != cudaSuccess) return sbr::cuda_fail(e__, #call); \
+    } while (0)
+
+// Device-side error word bits (written by kernels, read after each execute).
+enum : uint32_t {
+    DEV_ERR_STACK = 1u,      // traversal stack would overflow (entry dropped)
+    DEV_ERR_BUDGET = 2u,     // per-query iteration budget exceeded
+    DEV_ERR_CANCEL = 4u,     // cancel flag observed
+};
+
+// ------------------------------------------------------------- GPU layout
+// Binary BVH with both child boxes stored in the parent (one 64 B node = four
+// 16 B loads).  Child reference: >= 0 inner node index; < 0 leaf, where
+// ~ref = first_triangle * 16 + count (count 1..15).
+struct __align__(16) GNode {
+    float4 a;     // child 0: lo.x hi.x lo.y hi.y
+    float4 b;     // child 1: lo.x hi.x lo.y hi.y
+    float4 c;     // child 0 lo.z hi.z, child 1 lo.z hi.z
+    int4 link;    // ref0, ref1, unused, unused
+};
+static_assert(sizeof(GNode) == 64, "GNode must be 64 bytes");
+
+constexpr int kLeafMax = 15;
+constexpr int kStackDepth = 64;     // reference uses 64 (src/cuda/rtKernels.cu:65)
+
+// Leaf-ordered triangle: v0, e1 = v1 - v0, e2 = v2 - v0 and the unit normal
+// unit(e1 x e2) in the w lanes (three 16 B loads).
+struct __align__(16) GTri {
+    float4 p;     // v0.xyz, n.x
+    float4 e1;    // e1.xyz, n.y
+    float4 e2;    // e2.xyz, n.z
+};
+
+// FP64 twin of GTri used by SBR_PREC_FP64.
+struct GTri64 {
+    double v0[3], e1[3], e2[3], n[3];
+};
+
+struct SceneView {
+    const GNode* __restrict__ nodes;
+    const GTri* __restrict__ tris;
+    const GTri64* __restrict__ tris64;
+    const int32_t* __restrict__ tri_id;
+};
+
+// --------------------------------------------------------------- plan data
+// One (job, angle) of a plan.  Frames are computed on the host in FP64.
+struct __align__(16) Segment {
+    double dir[3];        // incidence direction (toward the launcher)
+    double llc[3];        // launch corner used by this plan (reference corner at 10 G, minus shift * dir)
+    double u[3], v[3];    // launcher edge vectors (length G)
+    double shift;         // distance the launch plane was moved toward the scene (added back to the path)
+    float llcf[3];        // FP32 launch corner
+    float uf[3], vf[3];   // FP32 edge vectors
+    float rdf[3];         // FP32 ray direction (-dir)
+    int32_t job;          // job index
+    int32_t angle;        // angle index within the job
+    int32_t i0, j0;       // first ray (pixel) of the clipped rectangle
+    int32_t ni, nj;       // clipped rectangle size in rays
+    int32_t tiles_x;      // tiles across the clipped rectangle
+    int32_t tiles;        // tiles in the clipped rectangle
+    int32_t tiles_per_item;
+    int32_t pad;
+    int64_t item_base;    // first work item of this segment
+    int64_t sample_base;  // first output sample (angle, freq) index
+};
+struct JobConst {
+    int32_t nx, ny;
+    int32_t n_freqs;
+    int32_t max_bounces;
+    int32_t freq_base;    // index of this job's first frequency in the frequency table
+    int32_t pad;
+    double inv_nx, inv_ny;
+    double refl;          // reflection coefficient R
+    float reflf;
+    float pad2;
+};
+
+// Per frequency: k, the PO scale k*A/(4 pi) (ray area of the owning job), the
+// fixed-point quantum of the field accumulators, and FP32 copies used by the
+// reference FP32 arithmetic.
+struct FreqConst {
+    double k;
+    double scale;         // k * rayArea / (4 pi)
+    double quantum;       // field value of one accumulator unit
+    double inv_quantum;
+    float kf;
+    float scalef;
+};
+
+struct ItemStats {
+    uint32_t rays, hit_rays, bounces, queries;
+};
+
+// Tile of rays owned by one CTA work item: 16 x 16 rays, 256 threads; warp w
+// covers an 8 x 4 block at ((w & 1) * 8, (w >> 1) * 4).
+constexpr int kTileW = 16;
+constexpr int kTileH = 16;
+constexpr int kCtaThreads = kTileW * kTileH;
+
+}  // namespace sbr

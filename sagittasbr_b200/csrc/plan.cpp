@@ -1,0 +1,436 @@
+// plan.cpp -- sbr_plan: launcher frames, aperture clipping, the work-item table
+// and the device result buffers; execute / results / run.
+//
+// The per-angle launcher frame restates src/app/sweep.cu:342-364
+//   dir = (sin t cos p, sin t sin p, cos t), rayDir = -dir,
+//   up = (0,1,0) or (1,0,0) when |dir.y| > 0.99,
+//   U = unit(up x dir) G, V = unit(dir x U) G, llc = 10 G dir - U/2 - V/2,
+// and k / ray area restate src/app/sweep.cu:50-53.  Two things are added:
+//  * aperture clipping: rays whose (s, t) launcher coordinates fall outside the
+//    projection of the scene's bounding box cannot hit anything (their hit count
+//    stays 0 and they add nothing to the PO sum), so only the clipped rectangle of
+//    pixels (plus a one-pixel margin) is launched;
+//  * in SBR_PREC_MIXED the launch plane is moved from 10 G to just outside the
+//    scene along dir and the distance moved is added back to the FP64 path, which
+//    keeps FP32 ray coordinates small.  The first-hit tMin test is unchanged
+//    because no geometry lies between the two planes.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "plan.hpp"
+
+using namespace sbr;
+
+namespace {
+
+template <class R>
+struct Fr {
+    R dir[3], u[3], v[3], llc[3];
+};
+
+template <class R>
+Fr<R> frame(double thetaDeg, double phiDeg, R G) {
+    const R pi = R(M_PI);
+    R th = R(thetaDeg) * pi / R(180.0);
+    R ph = R(phiDeg) * pi / R(180.0);
+    Fr<R> f;
+    f.dir[0] = std::sin(th) * std::cos(ph);
+    f.dir[1] = std::sin(th) * std::sin(ph);
+    f.dir[2] = std::cos(th);
+    R up[3] = {R(0), R(1), R(0)};
+    if (std::fabs(f.dir[1]) > R(0.99)) { up[0] = R(1); up[1] = R(0); }
+    auto crs = [](const R* a, const R* b, R* o) {
+        o[0] = a[1] * b[2] - a[2] * b[1];
+        o[1] = -(a[0] * b[2] - a[2] * b[0]);
+        o[2] = a[0] * b[1] - a[1] * b[0];
+    };
+    auto unitScale = [](R* a, R G) {
+        R l = std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+        for (int k = 0; k < 3; ++k) a[k] = (a[k] / l) * G;
+    };
+    crs(up, f.dir, f.u);
+    unitScale(f.u, G);
+    crs(f.dir, f.u, f.v);
+    unitScale(f.v, G);
+    for (int k = 0; k < 3; ++k) f.llc[k] = (R(10.0) * G) * f.dir[k] - R(0.5) * f.u[k] - R(0.5) * f.v[k];
+    return f;
+}
+
+template <class T>
+sbr_status upload(T** d, const std::vector<T>& h, int64_t& bytes) {
+    size_t n = std::max<size_t>(h.size(), 1) * sizeof(T);
+    cudaError_t e = cudaMalloc(d, n);
+    if (e != cudaSuccess) return fail(SBR_ERR_OOM, "plan allocation failed");
+    bytes += (int64_t)n;
+    if (!h.empty()) SBR_CUDA(cudaMemcpy(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return SBR_OK;
+}
+
+template <class T>
+sbr_status zalloc(T** d, size_t count, int64_t& bytes) {
+    size_t n = std::max<size_t>(count, 1) * sizeof(T);
+    cudaError_t e = cudaMalloc(d, n);
+    if (e != cudaSuccess) return fail(SBR_ERR_OOM, "plan allocation failed");
+    bytes += (int64_t)n;
+    SBR_CUDA(cudaMemset(*d, 0, n));
+    return SBR_OK;
+}
+
+void release(sbr_plan* p) {
+    if (!p) return;
+    cudaSetDevice(p->scene->device);
+    if (p->stream) cudaStreamSynchronize(p->stream);
+    if (p->graph) cudaGraphExecDestroy(p->graph);
+    cudaFree(p->d_segs);
+    cudaFree(p->d_seg_base);
+    cudaFree(p->d_jobs);
+    cudaFree(p->d_freqs);
+    cudaFree(p->d_quantum);
+    cudaFree(p->d_acc);
+    cudaFree(p->d_acc_stats);
+    cudaFree(p->d_field);
+    cudaFree(p->d_stats);
+    cudaFree(p->d_queue);
+    if (p->ev0) cudaEventDestroy(p->ev0);
+    if (p->ev1) cudaEventDestroy(p->ev1);
+    delete p;
+}
+
+sbr_status check_device_errors(sbr_plan* p) {
+    uint32_t e = 0;
+    SBR_CUDA(cudaMemcpy(&e, p->d_err, sizeof(e), cudaMemcpyDeviceToHost));
+    if (e) SBR_CUDA(cudaMemset(p->d_err, 0, sizeof(e)));
+    if (e & DEV_ERR_CANCEL) return fail(SBR_ERR_CANCELLED, "run cancelled");
+    if (e & DEV_ERR_BUDGET) return fail(SBR_ERR_TIMEOUT, "traversal iteration budget exceeded");
+    if (e & DEV_ERR_STACK) return fail(SBR_ERR_STACK, "traversal stack overflow");
+    return SBR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+sbr_status sbr_plan_create(sbr_scene* s, const sbr_job* jobs, size_t n_jobs, const sbr_run_opts* opts,
+                           sbr_plan** out) {
+    if (!out) return fail(SBR_ERR_INVALID_ARG, "out is null");
+    *out = nullptr;
+    if (!s || (!jobs && n_jobs)) return fail(SBR_ERR_INVALID_ARG, "null scene or jobs");
+    sbr_run_opts o{};
+    if (opts) o = *opts;
+    if (o.mode != SBR_MODE_BATCHED && o.mode != SBR_MODE_PER_ANGLE) return fail(SBR_ERR_INVALID_ARG, "bad mode");
+    if (o.precision < SBR_PREC_MIXED || o.precision > SBR_PREC_FP64) return fail(SBR_ERR_INVALID_ARG, "bad precision");
+    if (o.polarization != SBR_POL_SCALAR) return fail(SBR_ERR_UNSUPPORTED, "polarisation tracking is not built");
+    for (size_t j = 0; j < n_jobs; ++j) {
+        const sbr_job& J = jobs[j];
+        if (J.n_angles < 0 || (J.n_angles > 0 && (!J.theta_deg || !J.phi_deg)))
+            return fail(SBR_ERR_INVALID_ARG, "job angles");
+        if (J.n_freqs < 1 || !J.freq_hz) return fail(SBR_ERR_INVALID_ARG, "job needs at least one frequency");
+        if (J.n_freqs > max_freqs_per_job()) return fail(SBR_ERR_TOO_LARGE, "more than 128 frequencies in one job");
+        if (J.nx <= 0 || J.ny <= 0) return fail(SBR_ERR_INVALID_ARG, "n_x and n_y must be positive");
+        if ((int64_t)J.nx * (int64_t)J.ny > (int64_t(1) << 31) - 1)
+            return fail(SBR_ERR_TOO_LARGE, "more than 2^31-1 rays per angle");
+        if (J.max_bounces < 0) return fail(SBR_ERR_INVALID_ARG, "max_bounces < 0");
+        if (!(J.grid_size > 0) || !std::isfinite(J.grid_size)) return fail(SBR_ERR_INVALID_ARG, "grid_size");
+        if (!std::isfinite(J.reflection_const)) return fail(SBR_ERR_NONFINITE, "reflection_const");
+        for (int64_t a = 0; a < J.n_angles; ++a)
+            if (!std::isfinite(J.theta_deg[a]) || !std::isfinite(J.phi_deg[a]))
+                return fail(SBR_ERR_NONFINITE, "non-finite angle");
+        for (int64_t f = 0; f < J.n_freqs; ++f)
+            if (!(J.freq_hz[f] > 0) || !std::isfinite(J.freq_hz[f])) return fail(SBR_ERR_INVALID_ARG, "frequency");
+    }
+    SBR_CUDA(cudaSetDevice(s->device));
+    if (o.precision == SBR_PREC_FP64) {
+        sbr_status st = ensure_fp64(s);
+        if (st != SBR_OK) return st;
+    }
+
+    sbr_plan* p = new sbr_plan();
+    p->scene = s;
+    p->mode = o.mode;
+    p->prec = o.precision;
+    p->pol = o.polarization;
+    p->use_graph = o.use_graph;
+    p->ctas_per_sm = o.ctas_per_sm;
+    p->num_sms = s->num_sms;
+    p->stream = o.stream ? (cudaStream_t)o.stream : s->stream;
+    p->scene_view = s->view();
+    p->d_err = s->d_err;
+    p->d_cancel = s->d_cancel;
+
+    const double c0 = 299792458.0;
+    const double* lo = s->aabb_lo;
+    const double* hi = s->aabb_hi;
+    double diag = std::sqrt((hi[0] - lo[0]) * (hi[0] - lo[0]) + (hi[1] - lo[1]) * (hi[1] - lo[1]) +
+                            (hi[2] - lo[2]) * (hi[2] - lo[2]));
+    int64_t item = 0, sample = 0;
+    p->seg_base.push_back(0);
+    for (size_t j = 0; j < n_jobs; ++j) {
+        const sbr_job& J = jobs[j];
+        JobConst jc{};
+        jc.nx = J.nx;
+        jc.ny = J.ny;
+        jc.n_freqs = (int32_t)J.n_freqs;
+        jc.max_bounces = J.max_bounces;
+        jc.freq_base = (int32_t)p->freqs.size();
+        jc.inv_nx = 1.0 / double(J.nx);
+        jc.inv_ny = 1.0 / double(J.ny);
+        jc.refl = J.reflection_const;
+        jc.reflf = float(J.reflection_const);
+        p->jobs.push_back(jc);
+        p->k_max = std::max<int>(p->k_max, (int)J.n_freqs);
+        // k and the PO scale (src/app/sweep.cu:50-53); FP32 copies in FP32 arithmetic
+        const double G = J.grid_size;
+        const double area = (G * G) / double(int64_t(J.nx) * int64_t(J.ny));
+        const float Gf = float(G);
+        const float areaf = (Gf * Gf) / float(int64_t(J.nx) * int64_t(J.ny));
+        double rmax = std::pow(std::max(1.0, std::fabs(J.reflection_const)), double(J.max_bounces));
+        std::vector<double> quantum;
+        for (int64_t f = 0; f < J.n_freqs; ++f) {
+            FreqConst fc{};
+            double lambda = c0 / J.freq_hz[f];
+            fc.k = 2.0 * M_PI / lambda;
+            fc.scale = fc.k * area / (4.0 * M_PI);
+            float lambdaf = 299792458.0f / float(J.freq_hz[f]);
+            fc.kf = 2.0f * float(M_PI) / lambdaf;
+            fc.scalef = fc.kf * areaf / (4.0f * float(M_PI));
+            // |field| <= rays * k A/(4 pi) * 2 * max(1,R)^maxB; 2^60 units cover it with margin
+            double bound = double(int64_t(J.nx) * int64_t(J.ny)) * std::max(fc.scale, double(fc.scalef)) * 2.0 * rmax;
+            double q = bound / 1152921504606846976.0;  // 2^60
+            if (!std::isfinite(q) || !(q > 0)) {
+                release(p);
+                return fail(SBR_ERR_TOO_LARGE, "field bound overflows (reflection_const^max_bounces too large)");
+            }
+            fc.quantum = q;
+            fc.inv_quantum = 1.0 / q;
+            p->freqs.push_back(fc);
+            quantum.push_back(q);
+        }
+        for (int64_t a = 0; a < J.n_angles; ++a) {
+            Segment g{};
+            Fr<double> fd = frame<double>(J.theta_deg[a], J.phi_deg[a], G);
+            Fr<float> ff = frame<float>(J.theta_deg[a], J.phi_deg[a], Gf);
+            // clipped pixel rectangle: projection of the 8 box corners on (U, V)
+            double smin = INFINITY, smax = -INFINITY, tmin = INFINITY, tmax = -INFINITY, pmax = -INFINITY;
+            double uu = fd.u[0] * fd.u[0] + fd.u[1] * fd.u[1] + fd.u[2] * fd.u[2];
+            double vv = fd.v[0] * fd.v[0] + fd.v[1] * fd.v[1] + fd.v[2] * fd.v[2];
+            for (int c = 0; c < 8; ++c) {
+                double P[3] = {(c & 1) ? hi[0] : lo[0], (c & 2) ? hi[1] : lo[1], (c & 4) ? hi[2] : lo[2]};
+                double r[3] = {P[0] - fd.llc[0], P[1] - fd.llc[1], P[2] - fd.llc[2]};
+                double sc = (r[0] * fd.u[0] + r[1] * fd.u[1] + r[2] * fd.u[2]) / uu;
+                double tc = (r[0] * fd.v[0] + r[1] * fd.v[1] + r[2] * fd.v[2]) / vv;
+                smin = std::min(smin, sc); smax = std::max(smax, sc);
+                tmin = std::min(tmin, tc); tmax = std::max(tmax, tc);
+                pmax = std::max(pmax, P[0] * fd.dir[0] + P[1] * fd.dir[1] + P[2] * fd.dir[2]);
+            }
+            auto clampi = [](double x, int n) { return (int)std::min<double>(std::max<double>(x, -1.0), double(n)); };
+            int i0 = clampi(std::ceil(smin * J.nx - 0.5) - 1, J.nx), i1 = clampi(std::floor(smax * J.nx - 0.5) + 1, J.nx);
+            int j0 = clampi(std::ceil(tmin * J.ny - 0.5) - 1, J.ny), j1 = clampi(std::floor(tmax * J.ny - 0.5) + 1, J.ny);
+            i0 = std::max(i0, 0); j0 = std::max(j0, 0);
+            i1 = std::min(i1, J.nx - 1); j1 = std::min(j1, J.ny - 1);
+            g.i0 = i0;
+            g.j0 = j0;
+            g.ni = std::max(0, i1 - i0 + 1);
+            g.nj = std::max(0, j1 - j0 + 1);
+            if (J.max_bounces == 0) g.ni = g.nj = 0;
+            double shift = 0.0;
+            if (o.precision == SBR_PREC_MIXED) {
+                shift = 10.0 * G - pmax - (0.01 + 1e-3 * diag);
+                if (!(shift > 0)) shift = 0.0;
+            }
+            for (int k = 0; k < 3; ++k) {
+                g.dir[k] = fd.dir[k];
+                g.u[k] = fd.u[k];
+                g.v[k] = fd.v[k];
+                g.llc[k] = fd.llc[k] - shift * fd.dir[k];
+                if (o.precision == SBR_PREC_FP32) {
+                    g.llcf[k] = ff.llc[k];
+                    g.uf[k] = ff.u[k];
+                    g.vf[k] = ff.v[k];
+                    g.rdf[k] = -ff.dir[k];
+                } else {
+                    g.llcf[k] = float(g.llc[k]);
+                    g.uf[k] = float(fd.u[k]);
+                    g.vf[k] = float(fd.v[k]);
+                    g.rdf[k] = float(-fd.dir[k]);
+                }
+            }
+            g.shift = shift;
+            g.job = (int32_t)j;
+            g.angle = (int32_t)a;
+            int tx = (g.ni + kTileW - 1) / kTileW, ty = (g.nj + kTileH - 1) / kTileH;
+            g.tiles_x = tx;
+            g.tiles = tx * ty;
+            int tpi = 1;
+            if (o.mode == SBR_MODE_BATCHED) tpi = std::min(32, std::max(1, (g.tiles + 255) / 256));
+            g.tiles_per_item = tpi;
+            g.item_base = item;
+            g.sample_base = sample;
+            item += (g.tiles + tpi - 1) / tpi;
+            sample += J.n_freqs;
+            p->n_rays_clipped += (int64_t)g.ni * g.nj;
+            p->n_rays_grid += (int64_t)J.nx * J.ny;
+            for (double q : quantum) p->quantum.push_back(q);
+            p->segs.push_back(g);
+            p->seg_base.push_back(item);
+        }
+    }
+    p->n_segs = (int64_t)p->segs.size();
+    p->n_items = item;
+    p->n_samples = sample;
+    if (p->n_segs > INT32_MAX) {
+        release(p);
+        return fail(SBR_ERR_TOO_LARGE, "too many angles");
+    }
+
+    sbr_status st;
+    int64_t& b = p->device_bytes;
+    if ((st = upload(&p->d_segs, p->segs, b)) != SBR_OK || (st = upload(&p->d_seg_base, p->seg_base, b)) != SBR_OK ||
+        (st = upload(&p->d_jobs, p->jobs, b)) != SBR_OK || (st = upload(&p->d_freqs, p->freqs, b)) != SBR_OK ||
+        (st = upload(&p->d_quantum, p->quantum, b)) != SBR_OK ||
+        (st = zalloc(&p->d_acc, 2 * (size_t)p->n_samples, b)) != SBR_OK ||
+        (st = zalloc(&p->d_acc_stats, 4 * (size_t)p->n_segs, b)) != SBR_OK ||
+        (st = zalloc(&p->d_field, 2 * (size_t)p->n_samples, b)) != SBR_OK ||
+        (st = zalloc(&p->d_stats, 4 * (size_t)p->n_segs, b)) != SBR_OK ||
+        (st = zalloc(&p->d_queue, 1, b)) != SBR_OK) {
+        release(p);
+        return st;
+    }
+    cudaError_t e;
+    if ((e = cudaEventCreate(&p->ev0)) != cudaSuccess || (e = cudaEventCreate(&p->ev1)) != cudaSuccess) {
+        release(p);
+        return cuda_fail(e, "cudaEventCreate");
+    }
+    *out = p;
+    return SBR_OK;
+}
+
+sbr_status sbr_plan_execute(sbr_plan* p) {
+    if (!p) return fail(SBR_ERR_INVALID_ARG, "plan is null");
+    SBR_CUDA(cudaSetDevice(p->scene->device));
+    SBR_CUDA(cudaEventRecord(p->ev0, p->stream));
+    if (p->use_graph && p->mode == SBR_MODE_BATCHED) {
+        if (!p->graph) {
+            // size the persistent grid outside capture, then capture the launches
+            cudaGraph_t g;
+            SBR_CUDA(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
+            sbr_status st = plan_launch(p, false, nullptr);
+            cudaError_t e = cudaStreamEndCapture(p->stream, &g);
+            if (st != SBR_OK) return st;
+            if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+            e = cudaGraphInstantiate(&p->graph, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+        }
+        SBR_CUDA(cudaGraphLaunch(p->graph, p->stream));
+    } else {
+        sbr_status st = plan_launch(p, false, nullptr);
+        if (st != SBR_OK) return st;
+    }
+    SBR_CUDA(cudaEventRecord(p->ev1, p->stream));
+    p->executed = true;
+    return SBR_OK;
+}
+
+sbr_status sbr_plan_results(sbr_plan* p, sbr_result* out) {
+    if (!p || !out) return fail(SBR_ERR_INVALID_ARG, "null argument");
+    if (!p->executed) return fail(SBR_ERR_INVALID_ARG, "plan was not executed");
+    SBR_CUDA(cudaSetDevice(p->scene->device));
+    SBR_CUDA(cudaEventSynchronize(p->ev1));
+    sbr_status st = check_device_errors(p);
+    if (st != SBR_OK) return st;
+    float ms = 0.0f;
+    SBR_CUDA(cudaEventElapsedTime(&ms, p->ev0, p->ev1));
+    out->device_ms = ms;
+    std::vector<double> f(2 * (size_t)p->n_samples);
+    if (p->n_samples)
+        SBR_CUDA(cudaMemcpyAsync(f.data(), p->d_field, f.size() * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+    if (out->stats && p->n_segs)
+        SBR_CUDA(cudaMemcpyAsync(out->stats, p->d_stats, 4 * (size_t)p->n_segs * sizeof(uint64_t),
+                                 cudaMemcpyDeviceToHost, p->stream));
+    SBR_CUDA(cudaStreamSynchronize(p->stream));
+    for (int64_t i = 0; i < p->n_samples; ++i) {
+        double re = f[2 * i], im = f[2 * i + 1];
+        if (out->field) { out->field[2 * i] = re; out->field[2 * i + 1] = im; }
+        double sigma = 4.0 * M_PI * (re * re + im * im);
+        if (out->sigma_m2) out->sigma_m2[i] = sigma;
+        if (out->rcs_dbsm) out->rcs_dbsm[i] = 10.0 * std::log10(std::max(sigma, 1e-10));
+    }
+    return SBR_OK;
+}
+
+sbr_status sbr_plan_device_results(sbr_plan* p, const double** d_field, const uint64_t** d_stats) {
+    if (!p) return fail(SBR_ERR_INVALID_ARG, "plan is null");
+    if (d_field) *d_field = p->d_field;
+    if (d_stats) *d_stats = reinterpret_cast<const uint64_t*>(p->d_stats);
+    return SBR_OK;
+}
+
+sbr_status sbr_plan_info_get(const sbr_plan* p, sbr_plan_info* out) {
+    if (!p || !out) return fail(SBR_ERR_INVALID_ARG, "null argument");
+    out->n_samples = p->n_samples;
+    out->n_job_angles = p->n_segs;
+    out->n_items = p->n_items;
+    out->n_rays_clipped = p->n_rays_clipped;
+    out->n_rays_grid = p->n_rays_grid;
+    out->n_pol = 1;
+    int64_t launches = 1;
+    if (p->mode == SBR_MODE_BATCHED) launches += p->n_items > 0 ? 1 : 0;
+    else
+        for (size_t g = 0; g < p->segs.size(); ++g)
+            if (p->seg_base[g + 1] > p->seg_base[g]) launches += p->jobs[p->segs[g].job].n_freqs;
+    out->launches_per_execute = (int32_t)std::min<int64_t>(launches, INT32_MAX);
+    out->device_bytes = p->device_bytes;
+    out->h2d_bytes = (int64_t)(p->segs.size() * sizeof(Segment) + p->seg_base.size() * sizeof(int64_t) +
+                               p->jobs.size() * sizeof(JobConst) + p->freqs.size() * sizeof(FreqConst) +
+                               p->quantum.size() * sizeof(double));
+    out->d2h_bytes = (int64_t)(2 * p->n_samples * sizeof(double) + 4 * p->n_segs * sizeof(uint64_t) + sizeof(uint32_t));
+    return SBR_OK;
+}
+
+sbr_status sbr_plan_destroy(sbr_plan* p) {
+    if (!p) return fail(SBR_ERR_INVALID_ARG, "plan is null");
+    release(p);
+    return SBR_OK;
+}
+
+sbr_status sbr_run(sbr_scene* s, const sbr_job* jobs, size_t n_jobs, sbr_result* out, const sbr_run_opts* opts) {
+    if (!out) return fail(SBR_ERR_INVALID_ARG, "out is null");
+    sbr_plan* p = nullptr;
+    sbr_status st = sbr_plan_create(s, jobs, n_jobs, opts, &p);
+    if (st != SBR_OK) return st;
+    st = sbr_plan_execute(p);
+    if (st == SBR_OK) st = sbr_plan_results(p, out);
+    release(p);
+    return st;
+}
+
+sbr_status sbr_trace_records(sbr_scene* s, const sbr_job* job, const sbr_run_opts* opts, sbr_ray_record* out) {
+    if (!s || !job || !out) return fail(SBR_ERR_INVALID_ARG, "null argument");
+    sbr_plan* p = nullptr;
+    sbr_status st = sbr_plan_create(s, job, 1, opts, &p);
+    if (st != SBR_OK) return st;
+    long long n = (long long)job->n_angles * job->nx * job->ny;
+    sbr_ray_record* d = nullptr;
+    cudaError_t e = cudaMalloc(&d, std::max<long long>(n, 1) * sizeof(sbr_ray_record));
+    if (e != cudaSuccess) {
+        release(p);
+        return fail(SBR_ERR_OOM, "record buffer allocation failed");
+    }
+    st = fill_records(d, n, p->stream);
+    if (st == SBR_OK) st = plan_launch(p, true, d);
+    if (st == SBR_OK) {
+        e = cudaStreamSynchronize(p->stream);
+        if (e != cudaSuccess) st = cuda_fail(e, "trace records");
+    }
+    if (st == SBR_OK) st = check_device_errors(p);
+    if (st == SBR_OK && n > 0) {
+        e = cudaMemcpy(out, d, n * sizeof(sbr_ray_record), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) st = cuda_fail(e, "record copy");
+    }
+    cudaFree(d);
+    release(p);
+    return st;
+}
+
+}  // extern "C"

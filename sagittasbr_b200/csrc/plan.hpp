@@ -1,0 +1,86 @@
+// plan.hpp -- the opaque handles behind sbr_scene and sbr_plan.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <vector>
+
+#include "common.hpp"
+
+struct sbr_scene {
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t stream = nullptr;
+    int64_t ntris = 0;
+    double model_scale = 1.0;
+    double aabb_lo[3] = {0, 0, 0}, aabb_hi[3] = {0, 0, 0};  // conservative, FP64
+    // host copies kept for the FP64 upload and diagnostics
+    std::vector<float> xyz;          // caller vertices (unscaled)
+    std::vector<uint32_t> idx;
+    std::vector<int32_t> order;      // leaf slot -> caller triangle index
+    // device
+    sbr::GNode* d_nodes = nullptr;
+    int64_t n_gnodes = 0;
+    int64_t n_bin_nodes = 0;
+    sbr::GTri* d_tris = nullptr;
+    sbr::GTri64* d_tris64 = nullptr;
+    int32_t* d_tri_id = nullptr;
+    uint32_t* d_err = nullptr;
+    int32_t* h_cancel = nullptr;     // mapped pinned word
+    int32_t* d_cancel = nullptr;
+    int depth = 0;
+    double build_ms = 0.0;
+    int64_t device_bytes = 0;
+
+    sbr::SceneView view() const { return sbr::SceneView{d_nodes, d_tris, d_tris64, d_tri_id}; }
+};
+
+struct sbr_plan {
+    sbr_scene* scene = nullptr;
+    int mode = SBR_MODE_BATCHED;
+    int prec = SBR_PREC_MIXED;
+    int pol = SBR_POL_SCALAR;
+    int use_graph = 0;
+    int ctas_per_sm = 0;
+    int num_sms = 0;
+    cudaStream_t stream = nullptr;
+    sbr::SceneView scene_view{};
+
+    std::vector<sbr::Segment> segs;
+    std::vector<int64_t> seg_base;     // [n_segs + 1] first item of each segment
+    std::vector<sbr::JobConst> jobs;
+    std::vector<sbr::FreqConst> freqs;
+    std::vector<double> quantum;       // per sample
+    int64_t n_segs = 0, n_items = 0, n_samples = 0;
+    int64_t n_rays_clipped = 0, n_rays_grid = 0;
+    int k_max = 1;
+    int persistent_grid = 0;
+    int launches = 0;
+
+    // device
+    sbr::Segment* d_segs = nullptr;
+    int64_t* d_seg_base = nullptr;
+    sbr::JobConst* d_jobs = nullptr;
+    sbr::FreqConst* d_freqs = nullptr;
+    double* d_quantum = nullptr;
+    unsigned long long* d_acc = nullptr;
+    unsigned long long* d_acc_stats = nullptr;
+    double* d_field = nullptr;
+    unsigned long long* d_stats = nullptr;
+    unsigned long long* d_queue = nullptr;
+    uint32_t* d_err = nullptr;
+    const volatile int32_t* d_cancel = nullptr;
+    int64_t device_bytes = 0;
+
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    bool executed = false;
+};
+
+namespace sbr {
+sbr_status plan_launch(sbr_plan* pl, bool records, sbr_ray_record* d_records);
+sbr_status fill_records(sbr_ray_record* d, long long n, cudaStream_t st);
+int max_freqs_per_job();
+sbr_status ensure_fp64(sbr_scene* s);
+}  // namespace sbr

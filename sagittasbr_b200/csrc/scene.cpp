@@ -1,0 +1,273 @@
+// scene.cpp -- sbr_scene: mesh validation, BVH build, GPU layout and upload.
+//
+// Replaces the set-up half of runRcsApp (src/app/rtRcsEntry.cu:109-196):
+// index checks, de-indexing with the model scale, buildBvh, and the device copies
+// of triangles and nodes.  Errors are returned, never exit()-ed.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+
+#include "bvh_build.hpp"
+#include "plan.hpp"
+
+using namespace sbr;
+
+namespace {
+
+float round_down(double x) {
+    float f = float(x);
+    if (double(f) > x) f = std::nextafter(f, -INFINITY);
+    return f;
+}
+float round_up(double x) {
+    float f = float(x);
+    if (double(f) < x) f = std::nextafter(f, INFINITY);
+    return f;
+}
+
+// Triangle vertex in the reference FP32 build's arithmetic: float(position) * float(scale)
+// (src/app/rtRcsEntry.cu:137-145 with Real = float).
+inline void vert32(const float* xyz, uint32_t k, float sc, float out[3]) {
+    for (int a = 0; a < 3; ++a) out[a] = xyz[3 * k + a] * sc;
+}
+// ... and in the FP64 build's: double(position) * double(scale).
+inline void vert64(const float* xyz, uint32_t k, double sc, double out[3]) {
+    for (int a = 0; a < 3; ++a) out[a] = double(xyz[3 * k + a]) * sc;
+}
+
+void free_scene(sbr_scene* s) {
+    if (!s) return;
+    int cur = -1;
+    cudaGetDevice(&cur);
+    cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    cudaFree(s->d_nodes);
+    cudaFree(s->d_tris);
+    cudaFree(s->d_tris64);
+    cudaFree(s->d_tri_id);
+    cudaFree(s->d_err);
+    if (s->h_cancel) cudaFreeHost(s->h_cancel);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    if (cur >= 0) cudaSetDevice(cur);
+    delete s;
+}
+
+}  // namespace
+
+namespace sbr {
+
+sbr_status ensure_fp64(sbr_scene* s) {
+    if (s->d_tris64) return SBR_OK;
+    std::vector<GTri64> t64(s->ntris);
+    for (int64_t slot = 0; slot < s->ntris; ++slot) {
+        int32_t t = s->order[slot];
+        double a[3], b[3], c[3];
+        vert64(s->xyz.data(), s->idx[3 * t], s->model_scale, a);
+        vert64(s->xyz.data(), s->idx[3 * t + 1], s->model_scale, b);
+        vert64(s->xyz.data(), s->idx[3 * t + 2], s->model_scale, c);
+        GTri64& g = t64[slot];
+        for (int k = 0; k < 3; ++k) { g.v0[k] = a[k]; g.e1[k] = b[k] - a[k]; g.e2[k] = c[k] - a[k]; }
+        double nx = g.e1[1] * g.e2[2] - g.e1[2] * g.e2[1];
+        double ny = -(g.e1[0] * g.e2[2] - g.e1[2] * g.e2[0]);
+        double nz = g.e1[0] * g.e2[1] - g.e1[1] * g.e2[0];
+        double len = std::sqrt(nx * nx + ny * ny + nz * nz);
+        if (len > 0) { g.n[0] = nx / len; g.n[1] = ny / len; g.n[2] = nz / len; }
+        else { g.n[0] = g.n[1] = g.n[2] = 0.0; }
+    }
+    SBR_CUDA(cudaSetDevice(s->device));
+    size_t bytes = sizeof(GTri64) * t64.size();
+    cudaError_t e = cudaMalloc(&s->d_tris64, bytes);
+    if (e != cudaSuccess) return fail(SBR_ERR_OOM, "cudaMalloc of FP64 triangles failed");
+    SBR_CUDA(cudaMemcpy(s->d_tris64, t64.data(), bytes, cudaMemcpyHostToDevice));
+    s->device_bytes += (int64_t)bytes;
+    return SBR_OK;
+}
+
+}  // namespace sbr
+
+extern "C" {
+
+sbr_status sbr_scene_create(const float* xyz, size_t nverts, const uint32_t* tri_idx, size_t ntris,
+                            const sbr_build_opts* opts, sbr_scene** out) {
+    if (!out) return fail(SBR_ERR_INVALID_ARG, "out is null");
+    *out = nullptr;
+    if (ntris == 0) return fail(SBR_ERR_EMPTY_MESH, "mesh contains no triangles");
+    if (!xyz || !tri_idx || nverts == 0) return fail(SBR_ERR_INVALID_ARG, "null vertex or index array");
+    if (ntris > (size_t(1) << 27)) return fail(SBR_ERR_TOO_LARGE, "more than 2^27 triangles");
+    sbr_build_opts o{};
+    if (opts) o = *opts;
+    double scale = o.model_scale == 0.0 ? 1.0 : o.model_scale;
+    if (!std::isfinite(scale)) return fail(SBR_ERR_NONFINITE, "model scale is not finite");
+    for (size_t i = 0; i < 3 * ntris; ++i)
+        if (tri_idx[i] >= nverts) return fail(SBR_ERR_BAD_INDEX, "triangle index out of range");
+    for (size_t i = 0; i < 3 * nverts; ++i)
+        if (!std::isfinite(xyz[i])) return fail(SBR_ERR_NONFINITE, "non-finite vertex coordinate");
+
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(SBR_ERR_NO_DEVICE, "no CUDA device");
+    int dev = o.device;
+    if (dev < 0) SBR_CUDA(cudaGetDevice(&dev));
+    if (dev >= ndev) return fail(SBR_ERR_INVALID_ARG, "device ordinal out of range");
+    cudaDeviceProp prop;
+    SBR_CUDA(cudaGetDeviceProperties(&prop, dev));
+    if (prop.major < 10) return fail(SBR_ERR_NO_DEVICE, "libsbr is built for sm_100a (B200); device is older");
+    SBR_CUDA(cudaSetDevice(dev));
+
+    auto t0 = std::chrono::steady_clock::now();
+    sbr_scene* s = new sbr_scene();
+    s->device = dev;
+    s->num_sms = prop.multiProcessorCount;
+    s->ntris = (int64_t)ntris;
+    s->model_scale = scale;
+    s->xyz.assign(xyz, xyz + 3 * nverts);
+    s->idx.assign(tri_idx, tri_idx + 3 * ntris);
+
+    // per-triangle conservative boxes (cover both the FP32 and FP64 vertices)
+    const float sc32 = float(scale);
+    std::vector<float> lo(3 * ntris), hi(3 * ntris);
+    for (size_t t = 0; t < ntris; ++t) {
+        for (int a = 0; a < 3; ++a) { lo[3 * t + a] = INFINITY; hi[3 * t + a] = -INFINITY; }
+        for (int c = 0; c < 3; ++c) {
+            float p32[3];
+            double p64[3];
+            vert32(xyz, tri_idx[3 * t + c], sc32, p32);
+            vert64(xyz, tri_idx[3 * t + c], scale, p64);
+            for (int a = 0; a < 3; ++a) {
+                lo[3 * t + a] = std::min({lo[3 * t + a], p32[a], round_down(p64[a])});
+                hi[3 * t + a] = std::max({hi[3 * t + a], p32[a], round_up(p64[a])});
+            }
+        }
+    }
+    BuildOptions bo;
+    bo.leaf_size = o.leaf_size > 0 ? std::min(o.leaf_size, kLeafMax) : 4;
+    bo.bin_count = o.bin_count > 0 ? o.bin_count : 16;
+    bo.n_threads = o.n_threads;
+    bo.max_leaf = kLeafMax;
+    BinTree tree = build_sah(lo, hi, bo);
+    s->order = tree.order;
+    s->n_bin_nodes = (int64_t)tree.nodes.size();
+    s->depth = tree.depth;
+    for (int a = 0; a < 3; ++a) { s->aabb_lo[a] = tree.nodes[0].lo[a]; s->aabb_hi[a] = tree.nodes[0].hi[a]; }
+
+    // GPU nodes: inner binary nodes in pre-order, both child boxes per node
+    std::vector<GNode> g;
+    auto leafRef = [](const BinNode& b) { return ~(b.first * 16 + b.count); };
+    const float far = 1e30f;
+    if (tree.nodes[0].left < 0) {
+        const BinNode& r = tree.nodes[0];
+        GNode n;
+        n.a = make_float4(r.lo[0], r.hi[0], r.lo[1], r.hi[1]);
+        n.b = make_float4(far, far, far, far);
+        n.c = make_float4(r.lo[2], r.hi[2], far, far);
+        n.link = make_int4(leafRef(r), ~0, 0, 0);
+        g.push_back(n);
+    } else {
+        std::vector<int32_t> gi(tree.nodes.size(), -1);
+        int32_t c = 0;
+        for (size_t i = 0; i < tree.nodes.size(); ++i)
+            if (tree.nodes[i].left >= 0) gi[i] = c++;
+        g.resize(c);
+        for (size_t i = 0; i < tree.nodes.size(); ++i) {
+            const BinNode& p = tree.nodes[i];
+            if (p.left < 0) continue;
+            const BinNode& L = tree.nodes[p.left];
+            const BinNode& R = tree.nodes[p.right];
+            GNode n;
+            n.a = make_float4(L.lo[0], L.hi[0], L.lo[1], L.hi[1]);
+            n.b = make_float4(R.lo[0], R.hi[0], R.lo[1], R.hi[1]);
+            n.c = make_float4(L.lo[2], L.hi[2], R.lo[2], R.hi[2]);
+            n.link = make_int4(L.left >= 0 ? gi[p.left] : leafRef(L), R.left >= 0 ? gi[p.right] : leafRef(R), 0, 0);
+            g[gi[i]] = n;
+        }
+    }
+    s->n_gnodes = (int64_t)g.size();
+
+    // leaf-ordered triangles: v0, e1, e2 in FP32 (reference FP32 arithmetic) and
+    // the unit normal unit(e1 x e2) (src/cuda/rtKernels.cu:13-14,42)
+    std::vector<GTri> tr(ntris);
+    std::vector<int32_t> ids(ntris);
+    for (size_t slot = 0; slot < ntris; ++slot) {
+        int32_t t = s->order[slot];
+        ids[slot] = t;
+        float a[3], b[3], c[3];
+        vert32(xyz, tri_idx[3 * t], sc32, a);
+        vert32(xyz, tri_idx[3 * t + 1], sc32, b);
+        vert32(xyz, tri_idx[3 * t + 2], sc32, c);
+        float e1[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+        float e2[3] = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
+        float nx = e1[1] * e2[2] - e1[2] * e2[1];
+        float ny = -(e1[0] * e2[2] - e1[2] * e2[0]);
+        float nz = e1[0] * e2[1] - e1[1] * e2[0];
+        float len = std::sqrt(nx * nx + ny * ny + nz * nz);
+        float n[3] = {0.0f, 0.0f, 0.0f};
+        if (len > 0.0f) { n[0] = nx / len; n[1] = ny / len; n[2] = nz / len; }
+        tr[slot].p = make_float4(a[0], a[1], a[2], n[0]);
+        tr[slot].e1 = make_float4(e1[0], e1[1], e1[2], n[1]);
+        tr[slot].e2 = make_float4(e2[0], e2[1], e2[2], n[2]);
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    s->build_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+
+    auto bail = [&](sbr_status st) {
+        free_scene(s);
+        return st;
+    };
+    cudaError_t e;
+    size_t nb = sizeof(GNode) * g.size(), tb = sizeof(GTri) * tr.size(), ib = sizeof(int32_t) * ids.size();
+    if ((e = cudaMalloc(&s->d_nodes, nb)) != cudaSuccess || (e = cudaMalloc(&s->d_tris, tb)) != cudaSuccess ||
+        (e = cudaMalloc(&s->d_tri_id, ib)) != cudaSuccess || (e = cudaMalloc(&s->d_err, sizeof(uint32_t))) != cudaSuccess)
+        return bail(fail(SBR_ERR_OOM, std::string("device allocation failed: ") + cudaGetErrorString(e)));
+    if ((e = cudaMemcpy(s->d_nodes, g.data(), nb, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(s->d_tris, tr.data(), tb, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(s->d_tri_id, ids.data(), ib, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemset(s->d_err, 0, sizeof(uint32_t))) != cudaSuccess)
+        return bail(cuda_fail(e, "scene upload"));
+    if ((e = cudaHostAlloc(&s->h_cancel, sizeof(int32_t), cudaHostAllocMapped)) != cudaSuccess)
+        return bail(cuda_fail(e, "cudaHostAlloc(cancel)"));
+    *s->h_cancel = 0;
+    if ((e = cudaHostGetDevicePointer(&s->d_cancel, s->h_cancel, 0)) != cudaSuccess)
+        return bail(cuda_fail(e, "cudaHostGetDevicePointer(cancel)"));
+    if ((e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return bail(cuda_fail(e, "cudaStreamCreate"));
+    s->device_bytes = (int64_t)(nb + tb + ib);
+    if (o.want_fp64 > 0) {
+        sbr_status st = ensure_fp64(s);
+        if (st != SBR_OK) return bail(st);
+    }
+    *out = s;
+    return SBR_OK;
+}
+
+sbr_status sbr_scene_destroy(sbr_scene* scene) {
+    if (!scene) return fail(SBR_ERR_INVALID_ARG, "scene is null");
+    free_scene(scene);
+    return SBR_OK;
+}
+
+sbr_status sbr_scene_info_get(const sbr_scene* s, sbr_scene_info* out) {
+    if (!s || !out) return fail(SBR_ERR_INVALID_ARG, "null argument");
+    out->n_triangles = s->ntris;
+    out->n_nodes_bin = s->n_bin_nodes;
+    out->n_nodes_gpu = s->n_gnodes;
+    out->device_bytes = s->device_bytes;
+    for (int a = 0; a < 3; ++a) { out->aabb_lo[a] = s->aabb_lo[a]; out->aabb_hi[a] = s->aabb_hi[a]; }
+    out->build_ms = s->build_ms;
+    out->device = s->device;
+    out->bvh_depth = s->depth;
+    return SBR_OK;
+}
+
+sbr_status sbr_scene_cancel(sbr_scene* s) {
+    if (!s) return fail(SBR_ERR_INVALID_ARG, "scene is null");
+    *(volatile int32_t*)s->h_cancel = 1;
+    return SBR_OK;
+}
+
+sbr_status sbr_scene_reset_cancel(sbr_scene* s) {
+    if (!s) return fail(SBR_ERR_INVALID_ARG, "scene is null");
+    *(volatile int32_t*)s->h_cancel = 0;
+    return SBR_OK;
+}
+
+}  // extern "C"

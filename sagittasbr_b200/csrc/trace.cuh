@@ -1,0 +1,237 @@
+// trace.cuh -- device building blocks of the SBR path for sm_100a:
+// closest-hit traversal of the GNode BVH, the bounce loop with PEC reflection and
+// the reference's scalar PO exit-ray term.
+//
+// Semantics follow the reference per-ray routine:
+//   ray origin at pixel centres ................ src/cuda/rtKernels.cu:118-123
+//   closest hit with tMin = 1e-3, tMax = 1e20 ... src/cuda/rtKernels.cu:136
+//   Moller-Trumbore, two-sided, |det| < 1e-6 .... src/cuda/rtKernels.cu:10-44
+//   normal unit(e1 x e2) ........................ src/cuda/rtKernels.cu:42
+//   reflect d - 2 (d.n) n, nudge p + 1e-4 n ..... src/cuda/rtKernels.cu:146-152
+//   PO: R^n, cos = n.(-d_last) > 0, phase 2 k L, mag = k A / (4 pi) * 2 cos R^n,
+//       term (-mag sin, mag cos) ............... src/cuda/poKernels.cu:81-109
+// The traversal order differs from the reference (nearest child first, entries
+// beyond the current closest hit are skipped, 2-wide nodes); it returns the same
+// closest hit except for exact ties between triangles (shared edges), where the
+// reference keeps the last triangle tested.
+#pragma once
+
+#include "common.hpp"
+
+namespace sbr {
+
+// ------------------------------------------------------------ small vectors
+struct F3 {
+    float x, y, z;
+};
+struct D3 {
+    double x, y, z;
+};
+__device__ __forceinline__ F3 f3(float x, float y, float z) { return {x, y, z}; }
+__device__ __forceinline__ F3 operator+(F3 a, F3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ F3 operator-(F3 a, F3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ F3 operator*(float s, F3 a) { return {s * a.x, s * a.y, s * a.z}; }
+__device__ __forceinline__ float dot(F3 a, F3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ F3 cross(F3 a, F3 b) {
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ F3 unit(F3 a) {
+    float l = sqrtf(a.x * a.x + a.y * a.y + a.z * a.z);
+    return {__fdiv_rn(a.x, l), __fdiv_rn(a.y, l), __fdiv_rn(a.z, l)};
+}
+__device__ __forceinline__ D3 operator+(D3 a, D3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ D3 operator-(D3 a, D3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ D3 operator*(double s, D3 a) { return {s * a.x, s * a.y, s * a.z}; }
+__device__ __forceinline__ double dot(D3 a, D3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ D3 cross(D3 a, D3 b) {
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ D3 unit(D3 a) {
+    double l = sqrt(a.x * a.x + a.y * a.y + a.z * a.z);
+    return {a.x / l, a.y / l, a.z / l};
+}
+
+// Per-thread traversal counters.
+struct QueryCount {
+    uint32_t iters;
+};
+
+__device__ __forceinline__ float safe_inv(float d) {
+    return __frcp_rn(fabsf(d) > 1e-20f ? d : copysignf(1e-20f, d));
+}
+__device__ __forceinline__ double safe_inv(double d) { return 1.0 / (fabs(d) > 1e-200 ? d : copysign(1e-200, d)); }
+
+// Slab entry distance of one child box, +inf when missed.  Boxes are stored
+// conservatively; the exit is widened by a relative 2^-20 so rounding of the
+// FMA form never rejects a box the ray touches.
+__device__ __forceinline__ float slab_f(float lx, float hx, float ly, float hy, float lz, float hz, F3 inv, F3 oi,
+                                        float tMin, float tMax) {
+    float x0 = fmaf(lx, inv.x, -oi.x), x1 = fmaf(hx, inv.x, -oi.x);
+    float y0 = fmaf(ly, inv.y, -oi.y), y1 = fmaf(hy, inv.y, -oi.y);
+    float z0 = fmaf(lz, inv.z, -oi.z), z1 = fmaf(hz, inv.z, -oi.z);
+    float tn = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), tMin));
+    float tf = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), tMax));
+    return tn <= tf * 1.00000095367431640625f ? tn : __int_as_float(0x7f800000);
+}
+__device__ __forceinline__ double slab_d(double lx, double hx, double ly, double hy, double lz, double hz, D3 o,
+                                         D3 inv, double tMin, double tMax) {
+    double x0 = (lx - o.x) * inv.x, x1 = (hx - o.x) * inv.x;
+    double y0 = (ly - o.y) * inv.y, y1 = (hy - o.y) * inv.y;
+    double z0 = (lz - o.z) * inv.z, z1 = (hz - o.z) * inv.z;
+    double tn = fmax(fmax(fmin(x0, x1), fmin(y0, y1)), fmax(fmin(z0, z1), tMin));
+    double tf = fmin(fmin(fmax(x0, x1), fmax(y0, y1)), fmin(fmax(z0, z1), tMax));
+    return tn <= tf * (1.0 + 1e-12) ? tn : __longlong_as_double(0x7ff0000000000000LL);
+}
+
+// Moller-Trumbore in the reference's operation order (FP32).
+__device__ __forceinline__ bool mt_f(const GTri& T, F3 o, F3 d, float tMin, float tMax, float& t) {
+    F3 e1 = f3(T.e1.x, T.e1.y, T.e1.z), e2 = f3(T.e2.x, T.e2.y, T.e2.z);
+    F3 pv = cross(d, e2);
+    float det = dot(e1, pv);
+    if (fabsf(det) < 1.0e-6f) return false;
+    float inv = __frcp_rn(det);
+    F3 tv = o - f3(T.p.x, T.p.y, T.p.z);
+    float u = dot(tv, pv) * inv;
+    if (u < 0.0f || u > 1.0f) return false;
+    F3 qv = cross(tv, e1);
+    float v = dot(d, qv) * inv;
+    if (v < 0.0f || u + v > 1.0f) return false;
+    float tt = dot(e2, qv) * inv;
+    if (tt < tMin || tt > tMax) return false;
+    t = tt;
+    return true;
+}
+
+__device__ __forceinline__ bool mt_d(const GTri64& T, D3 o, D3 d, double tMin, double tMax, double& t) {
+    D3 e1{T.e1[0], T.e1[1], T.e1[2]}, e2{T.e2[0], T.e2[1], T.e2[2]};
+    D3 pv = cross(d, e2);
+    double det = dot(e1, pv);
+    if (fabs(det) < 1.0e-6) return false;
+    double inv = 1.0 / det;
+    D3 tv = o - D3{T.v0[0], T.v0[1], T.v0[2]};
+    double u = dot(tv, pv) * inv;
+    if (u < 0.0 || u > 1.0) return false;
+    D3 qv = cross(tv, e1);
+    double v = dot(d, qv) * inv;
+    if (v < 0.0 || u + v > 1.0) return false;
+    double tt = dot(e2, qv) * inv;
+    if (tt < tMin || tt > tMax) return false;
+    t = tt;
+    return true;
+}
+
+__device__ __forceinline__ GNode load_node(const GNode* p) {
+    GNode n;
+    n.a = __ldg(&p->a);
+    n.b = __ldg(&p->b);
+    n.c = __ldg(&p->c);
+    n.link = __ldg(&p->link);
+    return n;
+}
+
+constexpr uint32_t kIterBudget = 1u << 22;  // node + leaf steps per query before giving up
+
+// Closest hit along o + t d, t in [tMin, tBest].  Returns the leaf slot of the hit
+// triangle (or -1).  `err` collects DEV_ERR_* bits.
+template <bool kF64>
+struct Walker;
+
+template <>
+struct Walker<false> {
+    __device__ __forceinline__ static int closest(const SceneView& S, F3 o, F3 d, float tMin, float& tBest,
+                                                  uint32_t& err) {
+        F3 inv{safe_inv(d.x), safe_inv(d.y), safe_inv(d.z)};
+        F3 oi{o.x * inv.x, o.y * inv.y, o.z * inv.z};
+        int stRef[kStackDepth];
+        float stT[kStackDepth];
+        int sp = 0;
+        int ref = 0;
+        int best = -1;
+        uint32_t iters = 0;
+        while (true) {
+            if (++iters > kIterBudget) { err |= DEV_ERR_BUDGET; return -1; }
+            if (ref >= 0) {
+                GNode n = load_node(S.nodes + ref);
+                float t0 = slab_f(n.a.x, n.a.y, n.a.z, n.a.w, n.c.x, n.c.y, inv, oi, tMin, tBest);
+                float t1 = slab_f(n.b.x, n.b.y, n.b.z, n.b.w, n.c.z, n.c.w, inv, oi, tMin, tBest);
+                bool h0 = t0 <= tBest, h1 = t1 <= tBest;
+                if (h0 && h1) {
+                    bool f = t1 < t0;
+                    int nearRef = f ? n.link.y : n.link.x;
+                    int farRef = f ? n.link.x : n.link.y;
+                    float farT = f ? t0 : t1;
+                    if (sp < kStackDepth) { stRef[sp] = farRef; stT[sp] = farT; ++sp; }
+                    else err |= DEV_ERR_STACK;
+                    ref = nearRef;
+                    continue;
+                }
+                if (h0) { ref = n.link.x; continue; }
+                if (h1) { ref = n.link.y; continue; }
+            } else {
+                int code = ~ref;
+                int first = code >> 4, cnt = code & 15;
+                for (int k = 0; k < cnt; ++k) {
+                    float t;
+                    if (mt_f(S.tris[first + k], o, d, tMin, tBest, t)) { tBest = t; best = first + k; }
+                }
+            }
+            // pop the next entry that can still hold a closer hit
+            bool found = false;
+            while (sp > 0) {
+                --sp;
+                if (stT[sp] <= tBest) { ref = stRef[sp]; found = true; break; }
+            }
+            if (!found) return best;
+        }
+    }
+};
+
+template <>
+struct Walker<true> {
+    __device__ __forceinline__ static int closest(const SceneView& S, D3 o, D3 d, double tMin, double& tBest,
+                                                  uint32_t& err) {
+        D3 inv{safe_inv(d.x), safe_inv(d.y), safe_inv(d.z)};
+        int stRef[kStackDepth];
+        double stT[kStackDepth];
+        int sp = 0;
+        int ref = 0;
+        int best = -1;
+        uint32_t iters = 0;
+        while (true) {
+            if (++iters > kIterBudget) { err |= DEV_ERR_BUDGET; return -1; }
+            if (ref >= 0) {
+                GNode n = load_node(S.nodes + ref);
+                double t0 = slab_d(n.a.x, n.a.y, n.a.z, n.a.w, n.c.x, n.c.y, o, inv, tMin, tBest);
+                double t1 = slab_d(n.b.x, n.b.y, n.b.z, n.b.w, n.c.z, n.c.w, o, inv, tMin, tBest);
+                bool h0 = t0 <= tBest, h1 = t1 <= tBest;
+                if (h0 && h1) {
+                    bool f = t1 < t0;
+                    int nearRef = f ? n.link.y : n.link.x;
+                    int farRef = f ? n.link.x : n.link.y;
+                    double farT = f ? t0 : t1;
+                    if (sp < kStackDepth) { stRef[sp] = farRef; stT[sp] = farT; ++sp; }
+                    else err |= DEV_ERR_STACK;
+                    ref = nearRef;
+                    continue;
+                }
+                if (h0) { ref = n.link.x; continue; }
+                if (h1) { ref = n.link.y; continue; }
+            } else {
+                int code = ~ref;
+                int first = code >> 4, cnt = code & 15;
+                for (int k = 0; k < cnt; ++k) {
+                    double t;
+                    if (mt_d(S.tris64[first + k], o, d, tMin, tBest, t)) { tBest = t; best = first + k; }
+                }
+            }
+            bool found = false;
+            while (sp > 0) {
+                --sp;
+                if (stT[sp] <= tBest) { ref = stRef[sp]; found = true; break; }
+            }
+            if (!found) return best;
+        }
+    }
+};
+
+}  // namespace sbr

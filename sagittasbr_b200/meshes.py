@@ -1,0 +1,162 @@
+"""Seeded synthetic PEC meshes for the benchmark and test workloads.
+
+Every generator returns ``(verts float32 [V,3], tris uint32 [T,3])`` with the
+winding pointing toward the illuminated side (outward for closed bodies, into the
+octant for the trihedral's inner faces): the reference's PO term only counts hits
+whose geometric normal ``unit(e1 x e2)`` faces the incoming ray
+(src/cuda/poKernels.cu:92-94, src/cuda/rtKernels.cu:42), so winding changes
+results.  Meshes are centred on their bounding-box centre because the reference
+launcher square is centred on the world origin (src/app/sweep.cu:357-364).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+C0 = 299792458.0
+
+
+def _orient_outward(verts, tris, centre=None):
+    """Flip triangles whose normal points toward ``centre`` (closed convex-ish bodies)."""
+    v = verts.astype(np.float64)
+    c = v.mean(axis=0) if centre is None else np.asarray(centre, dtype=np.float64)
+    a, b, cc = v[tris[:, 0]], v[tris[:, 1]], v[tris[:, 2]]
+    n = np.cross(b - a, cc - a)
+    cen = (a + b + cc) / 3.0 - c
+    flip = np.einsum("ij,ij->i", n, cen) < 0
+    out = tris.copy()
+    out[flip, 1], out[flip, 2] = tris[flip, 2], tris[flip, 1]
+    return out
+
+
+def centre_on_aabb(verts):
+    v = np.asarray(verts, dtype=np.float64)
+    mid = 0.5 * (v.min(axis=0) + v.max(axis=0))
+    return (v - mid).astype(np.float32)
+
+
+def icosahedron():
+    p = (1.0 + math.sqrt(5.0)) / 2.0
+    raw = []
+    for s1 in (-1.0, 1.0):
+        for s2 in (-1.0, 1.0):
+            raw += [(0.0, s1, s2 * p), (s1, s2 * p, 0.0), (s2 * p, 0.0, s1)]
+    v = np.array(raw)
+    # faces: vertex triples that are mutually one edge (length 2) apart
+    d = np.linalg.norm(v[:, None] - v[None], axis=-1)
+    adj = np.abs(d - 2.0) < 1e-9
+    faces = []
+    for i in range(12):
+        for j in range(i + 1, 12):
+            if not adj[i, j]:
+                continue
+            for k in range(j + 1, 12):
+                if adj[i, k] and adj[j, k]:
+                    faces.append((i, j, k))
+    v = v / np.linalg.norm(v, axis=1, keepdims=True)
+    t = _orient_outward(v, np.array(faces, dtype=np.int64), centre=(0, 0, 0))
+    return v, t
+
+
+def icosphere(level: int = 5, radius: float = 1.0):
+    """Subdivided icosahedron: 20*4**level triangles on a sphere of ``radius``."""
+    v, t = icosahedron()
+    verts = [tuple(x) for x in v]
+    for _ in range(level):
+        cache = {}
+
+        def mid(a, b):
+            key = (a, b) if a < b else (b, a)
+            if key not in cache:
+                m = np.add(verts[a], verts[b]) * 0.5
+                m = m / np.linalg.norm(m)
+                cache[key] = len(verts)
+                verts.append(tuple(m))
+            return cache[key]
+
+        nt = []
+        for a, b, c in t:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nt += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        t = np.array(nt, dtype=np.int64)
+    V = np.array(verts) * radius
+    return V.astype(np.float32), t.astype(np.uint32)
+
+
+def _grid_plate(axis: int, offset: float, lo: float, hi: float, n: int):
+    """Square plate in the plane x[axis] = offset spanning [lo,hi]^2, n x n x 2 triangles,
+    normal along +axis.  Local coordinates a,b map to axes (axis+1)%3, (axis+2)%3."""
+    s = np.linspace(lo, hi, n + 1)
+    A, B = np.meshgrid(s, s, indexing="ij")  # A along a, B along b
+    P = np.zeros(((n + 1) * (n + 1), 3))
+    P[:, axis] = offset
+    P[:, (axis + 1) % 3] = A.ravel()
+    P[:, (axis + 2) % 3] = B.ravel()
+    idx = np.arange((n + 1) * (n + 1)).reshape(n + 1, n + 1)
+    p00 = idx[:-1, :-1].ravel()
+    p10 = idx[1:, :-1].ravel()
+    p11 = idx[1:, 1:].ravel()
+    p01 = idx[:-1, 1:].ravel()
+    t1 = np.stack([p00, p10, p11], axis=1)
+    t2 = np.stack([p00, p11, p01], axis=1)
+    T = np.empty((2 * n * n, 3), dtype=np.int64)
+    T[0::2] = t1
+    T[1::2] = t2
+    return P, T
+
+
+def trihedral(edge: float = 1.0, n: int = 100):
+    """Three orthogonal square plates meeting at the corner (-edge/2,)*3, normals
+    pointing into the +x,+y,+z octant; 3 * n*n*2 triangles."""
+    h = edge / 2.0
+    vs, ts, off = [], [], 0
+    for axis in range(3):
+        P, T = _grid_plate(axis, -h, -h, h, n)
+        vs.append(P)
+        ts.append(T + off)
+        off += P.shape[0]
+    return np.concatenate(vs).astype(np.float32), np.concatenate(ts).astype(np.uint32)
+
+
+def plate(size: float = 1.0, n: int = 1, axis: int = 2):
+    """Square plate in the plane through the origin normal to ``axis`` (facing +axis)."""
+    P, T = _grid_plate(axis, 0.0, -size / 2, size / 2, n)
+    return P.astype(np.float32), T.astype(np.uint32)
+
+
+def dihedral(edge: float = 1.0, n: int = 4):
+    """Two orthogonal plates (x = -edge/2 facing +x, y = -edge/2 facing +y)."""
+    h = edge / 2.0
+    vs, ts, off = [], [], 0
+    for axis in (0, 1):
+        P, T = _grid_plate(axis, -h, -h, h, n)
+        vs.append(P)
+        ts.append(T + off)
+        off += P.shape[0]
+    V = np.concatenate(vs)
+    return centre_on_aabb(V), np.concatenate(ts).astype(np.uint32)
+
+
+def box(size: float = 1.0):
+    """Axis-aligned cube of side ``size`` centred on the origin, 12 outward triangles."""
+    h = size / 2.0
+    V = np.array([[x, y, z] for x in (-h, h) for y in (-h, h) for z in (-h, h)])
+    quads = [(0, 1, 3, 2), (4, 6, 7, 5), (0, 4, 5, 1), (2, 3, 7, 6), (0, 2, 6, 4), (1, 5, 7, 3)]
+    T = []
+    for a, b, c, d in quads:
+        T += [(a, b, c), (a, c, d)]
+    T = _orient_outward(V, np.array(T, dtype=np.int64), centre=(0, 0, 0))
+    return V.astype(np.float32), T.astype(np.uint32)
+
+
+def bounding_radius(verts) -> float:
+    """Radius of the bounding sphere about the AABB centre."""
+    v = np.asarray(verts, dtype=np.float64)
+    mid = 0.5 * (v.min(axis=0) + v.max(axis=0))
+    return float(np.sqrt(((v - mid) ** 2).sum(axis=1).max()))
+
+
+def rays_for(freq_hz: float, grid_size: float, rays_per_wavelength: float = 10.0) -> int:
+    """n_x = n_y = ceil(rays_per_wavelength * G / lambda)."""
+    return int(math.ceil(rays_per_wavelength * grid_size * freq_hz / C0 - 1e-9))
