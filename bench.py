@@ -212,6 +212,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--angles", type=int, default=0,
+                    help="profile case: trace only this many angles, evenly spread over the sweep")
+    ap.add_argument("--no-per-angle", action="store_true", help="skip the per-angle mode measurement")
     ap.add_argument("--per-angle-stride", type=int, default=8,
                     help="per-angle mode is timed on every n-th angle of the sweep")
     args = ap.parse_args()
@@ -230,7 +233,14 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
     w = workload(rank)
-    stream = torch.cuda.current_stream()
+    if args.angles > 0:
+        pick = np.linspace(0, w["theta"].size - 1, args.angles).round().astype(int)
+        w["theta"], w["phi"] = w["theta"][pick], w["phi"][pick]
+        w["name"] += f"_subset{args.angles}"
+    # a real stream: the library treats a null handle as "its own stream", so the
+    # legacy default stream (handle 0) cannot be shared with torch's events
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     sp = stream.cuda_stream
     scene = sbr.Scene(w["verts"], w["tris"], device=local)
     job = sbr.JobSpec(w["theta"], w["phi"], w["freqs"], w["nx"], w["ny"], w["G"], w["max_bounces"], w["R"])
@@ -288,24 +298,30 @@ def main():
     assert np.array_equal(r2.field, res.field), "sbr_run and plan results differ"
 
     # per-angle mode (the reference's loop structure) on a subset of the same sweep
-    sub = slice(0, None, args.per_angle_stride)
-    pjob = sbr.JobSpec(w["theta"][sub], w["phi"][sub], w["freqs"], w["nx"], w["ny"], w["G"], w["max_bounces"], w["R"])
-    pplan = sbr.Plan(scene, [pjob], mode=sbr.MODE_PER_ANGLE, precision=sbr.PREC_FP32, stream=sp)
-    pplan.execute()
-    torch.cuda.synchronize()
-    pa0, pa1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    pa0.record(stream)
-    pplan.execute()
-    pa1.record(stream)
-    torch.cuda.synchronize()
-    pa_ms = pa0.elapsed_time(pa1)
-    per_angle_value = pplan.info["n_samples"] / (pa_ms * 1e-3)
-    pres = pplan.results()
-    bplan = sbr.Plan(scene, [pjob], mode=sbr.MODE_BATCHED, precision=sbr.PREC_MIXED, stream=sp)
-    bplan.execute()
-    bres = bplan.results()
-    with np.errstate(divide="ignore"):
-        d_db = np.abs(pres.rcs_dbsm - bres.rcs_dbsm)
+    per_angle = None
+    if not args.no_per_angle:
+        sub = slice(0, None, args.per_angle_stride)
+        pjob = sbr.JobSpec(w["theta"][sub], w["phi"][sub], w["freqs"], w["nx"], w["ny"], w["G"], w["max_bounces"],
+                           w["R"])
+        pplan = sbr.Plan(scene, [pjob], mode=sbr.MODE_PER_ANGLE, precision=sbr.PREC_FP32, stream=sp)
+        pplan.execute()
+        torch.cuda.synchronize()
+        pa0, pa1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        pa0.record(stream)
+        pplan.execute()
+        pa1.record(stream)
+        torch.cuda.synchronize()
+        pa_ms = pa0.elapsed_time(pa1)
+        per_angle_value = pplan.info["n_samples"] / (pa_ms * 1e-3)
+        pres = pplan.results()
+        bplan = sbr.Plan(scene, [pjob], mode=sbr.MODE_BATCHED, precision=sbr.PREC_MIXED, stream=sp)
+        bplan.execute()
+        bres = bplan.results()
+        field_rel = float(np.abs(pres.field - bres.field).max() / np.abs(bres.field).max())
+        per_angle = {"value": per_angle_value, "unit": "samples/s", "precision": "fp32 (reference arithmetic)",
+                     "angles": pplan.info["n_samples"], "ms": pa_ms, "launches": pplan.info["launches_per_execute"],
+                     "max_field_err_vs_batched_rel_to_max": field_rel,
+                     "batched_speedup": value / ws / per_angle_value}
 
     if dist is not None:
         dist.barrier()
@@ -348,10 +364,7 @@ def main():
         "mray_bounces_per_s": bounces_step * ws / (step_ms * 1e-3) / 1e6,
         "closest_hit_queries_per_s": queries_step * ws / (step_ms * 1e-3),
         "kernel_ms": kern_ms,
-        "per_angle": {"value": per_angle_value, "unit": "samples/s", "precision": "fp32 (reference arithmetic)",
-                      "angles": pplan.info["n_samples"], "ms": pa_ms, "launches": pplan.info["launches_per_execute"],
-                      "max_abs_ddb_vs_batched": float(np.nanmax(d_db)),
-                      "batched_speedup": value / ws / per_angle_value},
+        "per_angle": per_angle,
         "e2e": {"value": e2e_value, "unit": "samples/s", "h2d_bytes_per_step": info["h2d_bytes"],
                 "d2h_bytes_per_step": info["d2h_bytes"], "ms_per_step": float(e2e_t[0])},
         "gpu_launches": int(info["launches_per_execute"]) * args.steps,

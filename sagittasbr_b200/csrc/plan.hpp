@@ -27,8 +27,9 @@ struct sbr_scene {
     sbr::GTri64* d_tris64 = nullptr;
     int32_t* d_tri_id = nullptr;
     uint32_t* d_err = nullptr;
-    int32_t* h_cancel = nullptr;     // mapped pinned word
-    int32_t* d_cancel = nullptr;
+    int32_t* d_cancel = nullptr;     // device word polled by the kernels
+    int32_t* h_flag_vals = nullptr;  // pinned {1, 0}: sources of the async flag copies
+    cudaStream_t cancel_stream = nullptr;
     int depth = 0;
     double build_ms = 0.0;
     int64_t device_bytes = 0;

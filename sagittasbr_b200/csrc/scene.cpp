@@ -47,7 +47,9 @@ void free_scene(sbr_scene* s) {
     cudaFree(s->d_tris64);
     cudaFree(s->d_tri_id);
     cudaFree(s->d_err);
-    if (s->h_cancel) cudaFreeHost(s->h_cancel);
+    cudaFree(s->d_cancel);
+    if (s->h_flag_vals) cudaFreeHost(s->h_flag_vals);
+    if (s->cancel_stream) cudaStreamDestroy(s->cancel_stream);
     if (s->stream) cudaStreamDestroy(s->stream);
     if (cur >= 0) cudaSetDevice(cur);
     delete s;
@@ -223,12 +225,17 @@ sbr_status sbr_scene_create(const float* xyz, size_t nverts, const uint32_t* tri
         (e = cudaMemcpy(s->d_tri_id, ids.data(), ib, cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemset(s->d_err, 0, sizeof(uint32_t))) != cudaSuccess)
         return bail(cuda_fail(e, "scene upload"));
-    if ((e = cudaHostAlloc(&s->h_cancel, sizeof(int32_t), cudaHostAllocMapped)) != cudaSuccess)
-        return bail(cuda_fail(e, "cudaHostAlloc(cancel)"));
-    *s->h_cancel = 0;
-    if ((e = cudaHostGetDevicePointer(&s->d_cancel, s->h_cancel, 0)) != cudaSuccess)
-        return bail(cuda_fail(e, "cudaHostGetDevicePointer(cancel)"));
-    if ((e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) != cudaSuccess)
+    // cancel flag: a device word (the kernels poll it from L2); the host sets it with an
+    // asynchronous copy on a side stream, which runs while the sweep kernel is resident
+    if ((e = cudaMalloc(&s->d_cancel, sizeof(int32_t))) != cudaSuccess ||
+        (e = cudaMemset(s->d_cancel, 0, sizeof(int32_t))) != cudaSuccess)
+        return bail(cuda_fail(e, "cancel flag"));
+    if ((e = cudaHostAlloc(&s->h_flag_vals, 2 * sizeof(int32_t), cudaHostAllocDefault)) != cudaSuccess)
+        return bail(cuda_fail(e, "cudaHostAlloc(cancel values)"));
+    s->h_flag_vals[0] = 1;
+    s->h_flag_vals[1] = 0;
+    if ((e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&s->cancel_stream, cudaStreamNonBlocking)) != cudaSuccess)
         return bail(cuda_fail(e, "cudaStreamCreate"));
     s->device_bytes = (int64_t)(nb + tb + ib);
     if (o.want_fp64 > 0) {
@@ -260,13 +267,18 @@ sbr_status sbr_scene_info_get(const sbr_scene* s, sbr_scene_info* out) {
 
 sbr_status sbr_scene_cancel(sbr_scene* s) {
     if (!s) return fail(SBR_ERR_INVALID_ARG, "scene is null");
-    *(volatile int32_t*)s->h_cancel = 1;
+    SBR_CUDA(cudaSetDevice(s->device));
+    SBR_CUDA(cudaMemcpyAsync(s->d_cancel, &s->h_flag_vals[0], sizeof(int32_t), cudaMemcpyHostToDevice,
+                             s->cancel_stream));
     return SBR_OK;
 }
 
 sbr_status sbr_scene_reset_cancel(sbr_scene* s) {
     if (!s) return fail(SBR_ERR_INVALID_ARG, "scene is null");
-    *(volatile int32_t*)s->h_cancel = 0;
+    SBR_CUDA(cudaSetDevice(s->device));
+    SBR_CUDA(cudaMemcpyAsync(s->d_cancel, &s->h_flag_vals[1], sizeof(int32_t), cudaMemcpyHostToDevice,
+                             s->cancel_stream));
+    SBR_CUDA(cudaStreamSynchronize(s->cancel_stream));
     return SBR_OK;
 }
 

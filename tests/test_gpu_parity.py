@@ -97,7 +97,7 @@ def test_hit_sequences(brute, name, prec):
     np.testing.assert_array_equal(rec["tri"][ok], o["tri"][ok])
     hit = ok & (o["count"] > 0)
     tol = 1e-9 if prec == sbr.PREC_FP64 else 2e-5
-    np.testing.assert_allclose(rec["dist"][hit], o["dist"][hit], rtol=0, atol=tol * np.maximum(1, o["dist"][hit]))
+    assert np.all(np.abs(rec["dist"][hit] - o["dist"][hit]) <= tol * np.maximum(1.0, o["dist"][hit]))
     np.testing.assert_allclose(rec["normal"][hit], o["normal"][hit], atol=1e-5)
 
 
@@ -215,22 +215,42 @@ def test_sphere_sweep_against_oracle_and_mie(oracle):
                for p in (sbr.PREC_MIXED, sbr.PREC_FP64, sbr.PREC_FP32)}
     o = oracle.sweep(v, t, th, ph, [1e9], n, n, 2.0, 3, precision=64)
     ref_db = o.dbsm.ravel()
+    # At phi = 0, sin(phi) = 0 exactly: the middle ray row lies in the mesh's y = 0
+    # symmetry plane with d.y = -0, and the reference slab test evaluates 0 * inf =
+    # NaN for boxes with a face at y = 0 (src/cuda/rtKernels.cu:47-55), dropping
+    # them; its tree walk then misses hits that the closest-hit definition (brute
+    # force over every triangle) finds.  That angle is compared with brute force.
+    ob = oracle.sweep(v, t, [90.0], [0.0], [1e9], n, n, 2.0, 3, precision=64, accel="brute")
+    assert abs(ob.dbsm[0, 0] - ref_db[0]) > 0.1  # the reference walk's loss is real
+    ref_db[0] = ob.dbsm[0, 0]
     for p, r in res.items():
         assert np.max(np.abs(r.rcs_dbsm - ref_db)) <= 0.1, (p, np.max(np.abs(r.rcs_dbsm - ref_db)))
     sigma_mie = mie.sphere_rcs(1.0, 1e9)
     assert abs(np.mean(res[sbr.PREC_MIXED].sigma_m2) / sigma_mie - 1) < 0.1
 
 
-def test_trihedral_boresight_peak():
-    """Square trihedral, edge a = 1 m, 10 GHz, 578^2 rays: the triple-bounce
-    boresight return approaches the PO peak 12 pi a^4 / lambda^2."""
+def test_trihedral_full_resolution_against_oracle(oracle):
+    """Square trihedral, 60k triangles, 10 GHz, 578^2 rays, 3 bounces, at the
+    boresight and off it.  Compared with the FP64 oracle walking the reference
+    tree: |dS| <= 1e-3 * sum_r |term_r| (precision and edge flips together).
+    The reference's phase is 2 k times the summed path from the launcher
+    (src/cuda/poKernels.cu:95), not the retro-reflected round trip, so the
+    triple-bounce rays do not add in phase at the boresight as a physical
+    corner reflector's would; the oracle is the only pin."""
     v, t = M.trihedral(1.0, 100)
     G = 2.0 * M.bounding_radius(v)
     n = M.rays_for(1e10, G)
     assert n == 578
-    lam = C0 / 1e10
+    th, ph = [54.7356103172, 20.0], [45.0, 70.0]
     with sbr.Scene(v, t) as sc:
-        r = sbr.run(sc, sbr.JobSpec([54.7356103172], [45.0], [1e10], n, n, G, 3))
-    peak = 12 * np.pi / lam ** 2
-    assert abs(10 * np.log10(r.sigma_m2[0] / peak)) < 1.5
-    assert r.stats[0, 2] > 2.5 * r.stats[0, 1]  # mostly triple bounces
+        r = sbr.run(sc, sbr.JobSpec(th, ph, [1e10], n, n, G, 3))
+        recs = sbr.trace_records(sc, sbr.JobSpec(th, ph, [1e10], n, n, G, 3))
+    o = oracle.sweep(v, t, th, ph, [1e10], n, n, G, 3, precision=64, accel="tree")
+    k = 2 * np.pi * 1e10 / C0
+    scale = k * (G * G / (n * n)) / (4 * np.pi)
+    c = -(recs["normal"] * recs["lastdir"]).sum(axis=-1)
+    absum = scale * np.where((recs["count"] > 0) & (c > 0), 2 * c, 0).sum(axis=(1, 2))
+    assert np.all(np.abs(r.field - o.field.ravel()) <= 1e-3 * absum)
+    assert np.all(r.stats[:, 1] == o.counts["hit_rays"]) or \
+        np.all(np.abs(r.stats[:, 1].astype(float) - o.counts["hit_rays"]) <= 1e-4 * n * n)
+    assert r.stats[0, 2] > 2.5 * r.stats[0, 1]  # boresight: mostly triple bounces
