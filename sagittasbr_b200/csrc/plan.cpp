@@ -109,15 +109,10 @@ sbr_status check_device_errors(sbr_plan* p) {
 
 }  // namespace
 
-extern "C" {
+namespace sbr {
 
-sbr_status sbr_plan_create(sbr_scene* s, const sbr_job* jobs, size_t n_jobs, const sbr_run_opts* opts,
-                           sbr_plan** out) {
-    if (!out) return fail(SBR_ERR_INVALID_ARG, "out is null");
-    *out = nullptr;
+sbr_status validate_run(const sbr_scene* s, const sbr_job* jobs, size_t n_jobs, const sbr_run_opts& o) {
     if (!s || (!jobs && n_jobs)) return fail(SBR_ERR_INVALID_ARG, "null scene or jobs");
-    sbr_run_opts o{};
-    if (opts) o = *opts;
     if (o.mode != SBR_MODE_BATCHED && o.mode != SBR_MODE_PER_ANGLE) return fail(SBR_ERR_INVALID_ARG, "bad mode");
     if (o.precision < SBR_PREC_MIXED || o.precision > SBR_PREC_FP64) return fail(SBR_ERR_INVALID_ARG, "bad precision");
     if (o.polarization != SBR_POL_SCALAR) return fail(SBR_ERR_UNSUPPORTED, "polarisation tracking is not built");
@@ -139,32 +134,19 @@ sbr_status sbr_plan_create(sbr_scene* s, const sbr_job* jobs, size_t n_jobs, con
         for (int64_t f = 0; f < J.n_freqs; ++f)
             if (!(J.freq_hz[f] > 0) || !std::isfinite(J.freq_hz[f])) return fail(SBR_ERR_INVALID_ARG, "frequency");
     }
-    SBR_CUDA(cudaSetDevice(s->device));
-    if (o.precision == SBR_PREC_FP64) {
-        sbr_status st = ensure_fp64(s);
-        if (st != SBR_OK) return st;
-    }
+    return SBR_OK;
+}
 
-    sbr_plan* p = new sbr_plan();
-    p->scene = s;
-    p->mode = o.mode;
-    p->prec = o.precision;
-    p->pol = o.polarization;
-    p->use_graph = o.use_graph;
-    p->ctas_per_sm = o.ctas_per_sm;
-    p->num_sms = s->num_sms;
-    p->stream = o.stream ? (cudaStream_t)o.stream : s->stream;
-    p->scene_view = s->view();
-    p->d_err = s->d_err;
-    p->d_cancel = s->d_cancel;
-
+sbr_status build_tables(const sbr_scene* s, const sbr_job* jobs, size_t n_jobs, const sbr_run_opts& o,
+                        TableSink& sink, TableTotals& tot) {
     const double c0 = 299792458.0;
     const double* lo = s->aabb_lo;
     const double* hi = s->aabb_hi;
     double diag = std::sqrt((hi[0] - lo[0]) * (hi[0] - lo[0]) + (hi[1] - lo[1]) * (hi[1] - lo[1]) +
                             (hi[2] - lo[2]) * (hi[2] - lo[2]));
+    tot = TableTotals{};
     int64_t item = 0, sample = 0;
-    p->seg_base.push_back(0);
+    int32_t nfreq = 0;
     for (size_t j = 0; j < n_jobs; ++j) {
         const sbr_job& J = jobs[j];
         JobConst jc{};
@@ -172,20 +154,20 @@ sbr_status sbr_plan_create(sbr_scene* s, const sbr_job* jobs, size_t n_jobs, con
         jc.ny = J.ny;
         jc.n_freqs = (int32_t)J.n_freqs;
         jc.max_bounces = J.max_bounces;
-        jc.freq_base = (int32_t)p->freqs.size();
+        jc.freq_base = nfreq;
         jc.inv_nx = 1.0 / double(J.nx);
         jc.inv_ny = 1.0 / double(J.ny);
         jc.refl = J.reflection_const;
         jc.reflf = float(J.reflection_const);
-        p->jobs.push_back(jc);
-        p->k_max = std::max<int>(p->k_max, (int)J.n_freqs);
+        if (!sink.job(jc)) return fail(SBR_ERR_TOO_LARGE, "table capacity exceeded (jobs)");
+        tot.k_max = std::max<int>(tot.k_max, (int)J.n_freqs);
         // k and the PO scale (src/app/sweep.cu:50-53); FP32 copies in FP32 arithmetic
         const double G = J.grid_size;
         const double area = (G * G) / double(int64_t(J.nx) * int64_t(J.ny));
         const float Gf = float(G);
         const float areaf = (Gf * Gf) / float(int64_t(J.nx) * int64_t(J.ny));
         double rmax = std::pow(std::max(1.0, std::fabs(J.reflection_const)), double(J.max_bounces));
-        std::vector<double> quantum;
+        double quantum[128];
         for (int64_t f = 0; f < J.n_freqs; ++f) {
             FreqConst fc{};
             double lambda = c0 / J.freq_hz[f];
@@ -197,14 +179,13 @@ sbr_status sbr_plan_create(sbr_scene* s, const sbr_job* jobs, size_t n_jobs, con
             // |field| <= rays * k A/(4 pi) * 2 * max(1,R)^maxB; 2^60 units cover it with margin
             double bound = double(int64_t(J.nx) * int64_t(J.ny)) * std::max(fc.scale, double(fc.scalef)) * 2.0 * rmax;
             double q = bound / 1152921504606846976.0;  // 2^60
-            if (!std::isfinite(q) || !(q > 0)) {
-                release(p);
+            if (!std::isfinite(q) || !(q > 0))
                 return fail(SBR_ERR_TOO_LARGE, "field bound overflows (reflection_const^max_bounces too large)");
-            }
             fc.quantum = q;
             fc.inv_quantum = 1.0 / q;
-            p->freqs.push_back(fc);
-            quantum.push_back(q);
+            if (!sink.freq(fc)) return fail(SBR_ERR_TOO_LARGE, "table capacity exceeded (frequencies)");
+            quantum[f] = q;
+            ++nfreq;
         }
         for (int64_t a = 0; a < J.n_angles; ++a) {
             Segment g{};
@@ -268,20 +249,81 @@ sbr_status sbr_plan_create(sbr_scene* s, const sbr_job* jobs, size_t n_jobs, con
             g.sample_base = sample;
             item += (g.tiles + tpi - 1) / tpi;
             sample += J.n_freqs;
-            p->n_rays_clipped += (int64_t)g.ni * g.nj;
-            p->n_rays_grid += (int64_t)J.nx * J.ny;
-            for (double q : quantum) p->quantum.push_back(q);
-            p->segs.push_back(g);
-            p->seg_base.push_back(item);
+            tot.n_rays_clipped += (int64_t)g.ni * g.nj;
+            tot.n_rays_grid += (int64_t)J.nx * J.ny;
+            if (!sink.segment(g, item, quantum, (int)J.n_freqs))
+                return fail(SBR_ERR_TOO_LARGE, "table capacity exceeded (angles or samples)");
+            tot.n_segs += 1;
         }
     }
-    p->n_segs = (int64_t)p->segs.size();
-    p->n_items = item;
-    p->n_samples = sample;
-    if (p->n_segs > INT32_MAX) {
-        release(p);
-        return fail(SBR_ERR_TOO_LARGE, "too many angles");
+    tot.n_items = item;
+    tot.n_samples = sample;
+    if (tot.n_segs > INT32_MAX) return fail(SBR_ERR_TOO_LARGE, "too many angles");
+    return SBR_OK;
+}
+
+}  // namespace sbr
+
+namespace {
+
+// Collects the tables of a plan in its host vectors.
+struct PlanSink : sbr::TableSink {
+    sbr_plan* p;
+    explicit PlanSink(sbr_plan* pl) : p(pl) { p->seg_base.push_back(0); }
+    bool job(const JobConst& j) override { p->jobs.push_back(j); return true; }
+    bool freq(const FreqConst& f) override { p->freqs.push_back(f); return true; }
+    bool segment(const Segment& g, int64_t next_item, const double* q, int nf) override {
+        p->segs.push_back(g);
+        p->seg_base.push_back(next_item);
+        for (int f = 0; f < nf; ++f) p->quantum.push_back(q[f]);
+        return true;
     }
+};
+
+}  // namespace
+
+extern "C" {
+
+sbr_status sbr_plan_create(sbr_scene* s, const sbr_job* jobs, size_t n_jobs, const sbr_run_opts* opts,
+                           sbr_plan** out) {
+    if (!out) return fail(SBR_ERR_INVALID_ARG, "out is null");
+    *out = nullptr;
+    sbr_run_opts o{};
+    if (opts) o = *opts;
+    sbr_status vs = validate_run(s, jobs, n_jobs, o);
+    if (vs != SBR_OK) return vs;
+    SBR_CUDA(cudaSetDevice(s->device));
+    if (o.precision == SBR_PREC_FP64) {
+        sbr_status st = ensure_fp64(s);
+        if (st != SBR_OK) return st;
+    }
+
+    sbr_plan* p = new sbr_plan();
+    p->scene = s;
+    p->mode = o.mode;
+    p->prec = o.precision;
+    p->pol = o.polarization;
+    p->use_graph = o.use_graph;
+    p->ctas_per_sm = o.ctas_per_sm;
+    p->num_sms = s->num_sms;
+    p->stream = o.stream ? (cudaStream_t)o.stream : s->stream;
+    p->scene_view = s->view();
+    p->d_err = s->d_err;
+    p->d_cancel = s->d_cancel;
+
+    PlanSink sink(p);
+    TableTotals tot;
+    sbr_status bs = build_tables(s, jobs, n_jobs, o, sink, tot);
+    if (bs != SBR_OK) {
+        release(p);
+        return bs;
+    }
+    p->k_max = tot.k_max;
+    p->n_segs = tot.n_segs;
+    p->n_items = tot.n_items;
+    p->n_samples = tot.n_samples;
+    p->n_rays_clipped = tot.n_rays_clipped;
+    p->n_rays_grid = tot.n_rays_grid;
 
     sbr_status st;
     int64_t& b = p->device_bytes;

@@ -80,6 +80,29 @@ struct sbr_plan {
 };
 
 namespace sbr {
+
+// Receives the host tables of a sweep as build_tables produces them; a sink
+// returns false when it has no room left.
+struct TableSink {
+    virtual ~TableSink() = default;
+    virtual bool job(const JobConst& j) = 0;
+    virtual bool freq(const FreqConst& f) = 0;
+    // one (job, angle) segment, the first item of the next segment, and the job's
+    // per-frequency accumulator units (one per output sample of this segment)
+    virtual bool segment(const Segment& g, int64_t next_item, const double* quantum, int n_freqs) = 0;
+};
+
+struct TableTotals {
+    int64_t n_segs = 0, n_items = 0, n_samples = 0, n_rays_clipped = 0, n_rays_grid = 0;
+    int k_max = 1;
+};
+
+// Argument checks shared by every sweep entry point.
+sbr_status validate_run(const sbr_scene* s, const sbr_job* jobs, size_t n_jobs, const sbr_run_opts& o);
+// Launcher frames, aperture clipping, work items and fixed-point units of a sweep.
+sbr_status build_tables(const sbr_scene* s, const sbr_job* jobs, size_t n_jobs, const sbr_run_opts& o,
+                        TableSink& sink, TableTotals& tot);
+
 sbr_status plan_launch(sbr_plan* pl, bool records, sbr_ray_record* d_records);
 sbr_status fill_records(sbr_ray_record* d, long long n, cudaStream_t st);
 int max_freqs_per_job();
