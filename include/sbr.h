@@ -187,6 +187,44 @@ typedef struct sbr_ray_record {
 sbr_status sbr_trace_records(sbr_scene* scene, const sbr_job* job, const sbr_run_opts* opts,
                              sbr_ray_record* out);
 
+/* ---------------------------------------------------- allocation-free sweep */
+/* No counterpart in the reference.
+ *
+ * sbr_run_noalloc traces one job exactly like sbr_run (batched mode) but never
+ * allocates or frees device memory.  It is meant for callers that cannot call
+ * cudaMalloc while they run: programs that work inside a fixed device-memory
+ * budget handed out at start-up (a memory pool or caching allocator that already
+ * owns the free HBM, so a fresh allocation fails or fragments it), and programs
+ * whose other streams must not be stalled by the device-wide synchronisation
+ * that cudaFree (and often cudaMalloc) performs.
+ *
+ * The sweep's scratch -- launcher frames, work-item table, fixed-point field
+ * accumulators and work-queue head -- lives in one statically sized device array
+ * inside libsbr (SBR_NOALLOC_SCRATCH_BYTES, held by every GPU that loads the
+ * library until the process exits).  The caller passes the scene and the device
+ * output arrays: d_field [n_angles * n_freqs * 2] doubles (re, im) and, if not
+ * NULL, d_stats [n_angles * 4] uint64 (rays, hit rays, bounces, queries).
+ *
+ * Limits: one job, at most SBR_NOALLOC_MAX_ANGLES angles and
+ * SBR_NOALLOC_MAX_SAMPLES angle-frequency samples per call; larger requests return
+ * SBR_ERR_TOO_LARGE.  SBR_PREC_FP64 needs a scene created with want_fp64 = 1
+ * (uploading FP64 triangles later would allocate); SBR_MODE_PER_ANGLE returns
+ * SBR_ERR_UNSUPPORTED.
+ * Set-up: the first call on a device looks up the device address of the array
+ * (cudaGetSymbolAddress) with that device current; make that first call before
+ * any stream capture.
+ * Sharing: every call on a device uses the same array, which keeps the previous
+ * call's contents; each call clears the accumulators and queue it needs.  Calls
+ * whose GPU work overlapped would race on the array and corrupt each other's
+ * results, so the library serialises calls (one lock per process) and each call
+ * returns only after its stream has finished; it then returns the device error
+ * status. */
+#define SBR_NOALLOC_MAX_ANGLES 1024
+#define SBR_NOALLOC_MAX_SAMPLES 4096
+#define SBR_NOALLOC_SCRATCH_BYTES (448u * 1024u)
+sbr_status sbr_run_noalloc(sbr_scene* scene, const sbr_job* job, double* d_field, uint64_t* d_stats,
+                           const sbr_run_opts* opts);
+
 /* --------------------------------------------------------- entry surface */
 /* config.txt keys and defaults of include/app/config.hpp:8-25. */
 typedef struct sbr_config {

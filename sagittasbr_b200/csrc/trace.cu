@@ -516,3 +516,171 @@ sbr_status fill_records(sbr_ray_record* d, long long n, cudaStream_t st) {
 int max_freqs_per_job() { return kMaxK; }
 
 }  // namespace sbr
+
+// =========================================================================
+// Allocation-free sweep (sbr_run_noalloc).  No counterpart in the reference.
+//
+// For callers that may not allocate device memory while they run (a fixed
+// device-memory budget owned by a pool, or other streams that must not be
+// stalled by the synchronisation cudaMalloc / cudaFree perform).  The scratch a
+// sweep needs beyond the caller's scene and output arrays lives in one file-scope
+// device array of fixed size; host code reaches it only through the address
+// cudaGetSymbolAddress returns for the current device.
+// =========================================================================
+#include <mutex>
+
+namespace sbr {
+namespace {
+
+// Layout of the scratch array (device side) and of its host staging copy.
+struct NoallocTables {
+    Segment segs[SBR_NOALLOC_MAX_ANGLES];
+    int64_t seg_base[SBR_NOALLOC_MAX_ANGLES + 1];
+    JobConst job;
+    FreqConst freqs[kMaxK];
+    double quantum[SBR_NOALLOC_MAX_SAMPLES];
+};
+struct NoallocScratch {
+    NoallocTables tables;
+    unsigned long long acc[2 * SBR_NOALLOC_MAX_SAMPLES];
+    unsigned long long acc_stats[4 * SBR_NOALLOC_MAX_ANGLES];
+    unsigned long long queue;
+};
+static_assert(sizeof(NoallocScratch) <= SBR_NOALLOC_SCRATCH_BYTES, "scratch layout exceeds the stated size");
+
+// The scratch itself: every GPU that loads libsbr holds it until exit.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[SBR_NOALLOC_SCRATCH_BYTES];
+
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mu;                           // one call at a time per process
+void* g_noalloc_addr[kNoallocMaxDevices] = {};     // device address of the array, per device
+NoallocTables g_noalloc_host;                      // host staging (static: no heap use per call)
+
+// Collects the sweep tables straight into the fixed-size staging copy.
+struct NoallocSink : TableSink {
+    int n_jobs = 0, n_freqs = 0, n_segs = 0, n_samples = 0;
+    bool job(const JobConst& j) override {
+        if (n_jobs++ > 0) return false;
+        g_noalloc_host.job = j;
+        return true;
+    }
+    bool freq(const FreqConst& f) override {
+        if (n_freqs >= kMaxK) return false;
+        g_noalloc_host.freqs[n_freqs++] = f;
+        return true;
+    }
+    bool segment(const Segment& g, int64_t next_item, const double* q, int nf) override {
+        if (n_segs >= SBR_NOALLOC_MAX_ANGLES || n_samples + nf > SBR_NOALLOC_MAX_SAMPLES) return false;
+        g_noalloc_host.segs[n_segs] = g;
+        g_noalloc_host.seg_base[n_segs + 1] = next_item;
+        for (int f = 0; f < nf; ++f) g_noalloc_host.quantum[n_samples + f] = q[f];
+        n_samples += nf;
+        ++n_segs;
+        return true;
+    }
+};
+
+// Set-up, once per device and with that device current: the device address of
+// the scratch array.  (Host code must never pass g_noalloc_scratch itself to a
+// kernel: on the host that name denotes a host-side stand-in.)
+sbr_status noalloc_address(int dev, NoallocScratch** out) {
+    if (dev < 0 || dev >= kNoallocMaxDevices) return fail(SBR_ERR_UNSUPPORTED, "device ordinal too large");
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(noalloc scratch)");
+        g_noalloc_addr[dev] = p;
+    }
+    *out = reinterpret_cast<NoallocScratch*>(g_noalloc_addr[dev]);
+    return SBR_OK;
+}
+
+}  // namespace
+}  // namespace sbr
+
+extern "C" sbr_status sbr_run_noalloc(sbr_scene* s, const sbr_job* job, double* d_field, uint64_t* d_stats,
+                                      const sbr_run_opts* opts) {
+    using namespace sbr;
+    if (!s || !job || !d_field) return fail(SBR_ERR_INVALID_ARG, "scene, job and d_field are required");
+    sbr_run_opts o{};
+    if (opts) o = *opts;
+    if (o.mode != SBR_MODE_BATCHED) return fail(SBR_ERR_UNSUPPORTED, "the allocation-free sweep runs batched only");
+    sbr_status st = validate_run(s, job, 1, o);
+    if (st != SBR_OK) return st;
+    if (job->n_angles > SBR_NOALLOC_MAX_ANGLES)
+        return fail(SBR_ERR_TOO_LARGE, "allocation-free sweep: more than SBR_NOALLOC_MAX_ANGLES (1024) angles");
+    if (job->n_angles * job->n_freqs > SBR_NOALLOC_MAX_SAMPLES)
+        return fail(SBR_ERR_TOO_LARGE, "allocation-free sweep: more than SBR_NOALLOC_MAX_SAMPLES (4096) samples");
+    if (o.precision == SBR_PREC_FP64 && !s->d_tris64)
+        return fail(SBR_ERR_UNSUPPORTED, "allocation-free FP64 sweep needs a scene created with want_fp64 = 1");
+
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    SBR_CUDA(cudaSetDevice(s->device));
+    NoallocScratch* D = nullptr;
+    st = noalloc_address(s->device, &D);
+    if (st != SBR_OK) return st;
+
+    NoallocSink sink;
+    g_noalloc_host.seg_base[0] = 0;
+    TableTotals tot;
+    st = build_tables(s, job, 1, o, sink, tot);
+    if (st != SBR_OK) return st;
+
+    cudaStream_t stream = o.stream ? (cudaStream_t)o.stream : s->stream;
+    const size_t nseg = (size_t)sink.n_segs, nsamp = (size_t)sink.n_samples;
+    // tables in; accumulators, counters and queue head cleared (the array keeps the last call's contents)
+    SBR_CUDA(cudaMemcpyAsync(D->tables.segs, g_noalloc_host.segs, nseg * sizeof(Segment), cudaMemcpyHostToDevice,
+                             stream));
+    SBR_CUDA(cudaMemcpyAsync(D->tables.seg_base, g_noalloc_host.seg_base, (nseg + 1) * sizeof(int64_t),
+                             cudaMemcpyHostToDevice, stream));
+    SBR_CUDA(cudaMemcpyAsync(&D->tables.job, &g_noalloc_host.job, sizeof(JobConst), cudaMemcpyHostToDevice, stream));
+    SBR_CUDA(cudaMemcpyAsync(D->tables.freqs, g_noalloc_host.freqs, (size_t)sink.n_freqs * sizeof(FreqConst),
+                             cudaMemcpyHostToDevice, stream));
+    SBR_CUDA(cudaMemcpyAsync(D->tables.quantum, g_noalloc_host.quantum, nsamp * sizeof(double),
+                             cudaMemcpyHostToDevice, stream));
+    SBR_CUDA(cudaMemsetAsync(D->acc, 0, 2 * nsamp * sizeof(unsigned long long), stream));
+    SBR_CUDA(cudaMemsetAsync(D->acc_stats, 0, 4 * nseg * sizeof(unsigned long long), stream));
+    SBR_CUDA(cudaMemsetAsync(&D->queue, 0, sizeof(unsigned long long), stream));
+
+    if (tot.n_items > 0) {
+        const void* fn = pick_kernel(o.precision, tot.k_max > kRegK, false);
+        int occ = 0;
+        SBR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kCtaThreads, 0));
+        int per = o.ctas_per_sm > 0 ? o.ctas_per_sm : std::max(1, occ);
+        TraceParams p{};
+        p.S = s->view();
+        p.segs = D->tables.segs;
+        p.seg_item_base = D->tables.seg_base;
+        p.n_segs = (int32_t)nseg;
+        p.k_begin = 0;
+        p.k_count = 0;
+        p.count_stats = 1;
+        p.jobs = &D->tables.job;
+        p.freqs = D->tables.freqs;
+        p.item_begin = 0;
+        p.item_end = tot.n_items;
+        p.queue = &D->queue;
+        p.acc = D->acc;
+        p.acc_stats = D->acc_stats;
+        p.err = s->d_err;
+        p.cancel = s->d_cancel;
+        p.records = nullptr;
+        int grid = (int)std::min<long long>((long long)per * s->num_sms, tot.n_items);
+        st = launch_trace(fn, grid, stream, p);
+        if (st != SBR_OK) return st;
+    }
+    long long nmax = std::max<long long>(std::max<long long>((long long)nsamp, 4LL * (long long)nseg), 1);
+    k_finalize<<<(unsigned)((nmax + 255) / 256), 256, 0, stream>>>(
+        (long long)nsamp, D->tables.quantum, D->acc, d_field, d_stats ? 4LL * (long long)nseg : 0LL, D->acc_stats,
+        reinterpret_cast<unsigned long long*>(d_stats), &D->queue);
+    SBR_CUDA(cudaGetLastError());
+    SBR_CUDA(cudaStreamSynchronize(stream));
+
+    uint32_t e = 0;
+    SBR_CUDA(cudaMemcpy(&e, s->d_err, sizeof(e), cudaMemcpyDeviceToHost));
+    if (e) SBR_CUDA(cudaMemset(s->d_err, 0, sizeof(e)));
+    if (e & DEV_ERR_CANCEL) return fail(SBR_ERR_CANCELLED, "run cancelled");
+    if (e & DEV_ERR_BUDGET) return fail(SBR_ERR_TIMEOUT, "traversal iteration budget exceeded");
+    if (e & DEV_ERR_STACK) return fail(SBR_ERR_STACK, "traversal stack overflow");
+    return SBR_OK;
+}
