@@ -78,9 +78,9 @@ struct __align__(16) Segment {
     int32_t angle;        // angle index within the job
     int32_t i0, j0;       // first ray (pixel) of the clipped rectangle
     int32_t ni, nj;       // clipped rectangle size in rays
-    int32_t tiles_x;      // tiles across the clipped rectangle
-    int32_t tiles;        // tiles in the clipped rectangle
-    int32_t tiles_per_item;
+    int32_t blocks_x;     // 8x4-ray blocks across the clipped rectangle
+    int32_t blocks;       // blocks in the clipped rectangle
+    int32_t blocks_per_item;
     int32_t pad;
     int64_t item_base;    // first work item of this segment
     int64_t sample_base;  // first output sample (angle, freq) index
@@ -113,10 +113,12 @@ struct ItemStats {
     uint32_t rays, hit_rays, bounces, queries;
 };
 
-// Tile of rays owned by one CTA work item: 16 x 16 rays, 256 threads; warp w
-// covers an 8 x 4 block at ((w & 1) * 8, (w >> 1) * 4).
-constexpr int kTileW = 16;
-constexpr int kTileH = 16;
-constexpr int kCtaThreads = kTileW * kTileH;
+// Rays are handed out in blocks of 8 x 4 pixels (one warp's worth of spatially
+// adjacent, parallel rays); a work item is a run of consecutive blocks of one
+// segment, owned by one warp.
+constexpr int kBlockW = 8;
+constexpr int kBlockH = 4;
+constexpr int kCtaThreads = 128;     // 4 independent warps per CTA
+constexpr int kAccReplicas = 8;      // copies of each accumulator (spreads same-address atomics)
 
 }  // namespace sbr

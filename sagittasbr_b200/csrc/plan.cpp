@@ -239,15 +239,17 @@ sbr_status build_tables(const sbr_scene* s, const sbr_job* jobs, size_t n_jobs, 
             g.shift = shift;
             g.job = (int32_t)j;
             g.angle = (int32_t)a;
-            int tx = (g.ni + kTileW - 1) / kTileW, ty = (g.nj + kTileH - 1) / kTileH;
-            g.tiles_x = tx;
-            g.tiles = tx * ty;
-            int tpi = 1;
-            if (o.mode == SBR_MODE_BATCHED) tpi = std::min(32, std::max(1, (g.tiles + 255) / 256));
-            g.tiles_per_item = tpi;
+            int bx = (g.ni + kBlockW - 1) / kBlockW, by = (g.nj + kBlockH - 1) / kBlockH;
+            g.blocks_x = bx;
+            g.blocks = bx * by;
+            // up to 8 blocks (256 rays) per warp item in batched mode, fewer when a
+            // segment is small; one block per item in per-angle mode, where a single
+            // segment must spread over the whole GPU
+            int bpi = o.mode == SBR_MODE_BATCHED ? std::max(1, std::min(8, g.blocks / 1024)) : 1;
+            g.blocks_per_item = bpi;
             g.item_base = item;
             g.sample_base = sample;
-            item += (g.tiles + tpi - 1) / tpi;
+            item += (g.blocks + bpi - 1) / bpi;
             sample += J.n_freqs;
             tot.n_rays_clipped += (int64_t)g.ni * g.nj;
             tot.n_rays_grid += (int64_t)J.nx * J.ny;
@@ -330,11 +332,11 @@ sbr_status sbr_plan_create(sbr_scene* s, const sbr_job* jobs, size_t n_jobs, con
     if ((st = upload(&p->d_segs, p->segs, b)) != SBR_OK || (st = upload(&p->d_seg_base, p->seg_base, b)) != SBR_OK ||
         (st = upload(&p->d_jobs, p->jobs, b)) != SBR_OK || (st = upload(&p->d_freqs, p->freqs, b)) != SBR_OK ||
         (st = upload(&p->d_quantum, p->quantum, b)) != SBR_OK ||
-        (st = zalloc(&p->d_acc, 2 * (size_t)p->n_samples, b)) != SBR_OK ||
+        (st = zalloc(&p->d_acc, 2 * (size_t)p->n_samples * kAccReplicas, b)) != SBR_OK ||
         (st = zalloc(&p->d_acc_stats, 4 * (size_t)p->n_segs, b)) != SBR_OK ||
         (st = zalloc(&p->d_field, 2 * (size_t)p->n_samples, b)) != SBR_OK ||
         (st = zalloc(&p->d_stats, 4 * (size_t)p->n_segs, b)) != SBR_OK ||
-        (st = zalloc(&p->d_queue, 1, b)) != SBR_OK) {
+        (st = zalloc(&p->d_queue, 1 + (size_t)p->n_samples, b)) != SBR_OK) {
         release(p);
         return st;
     }

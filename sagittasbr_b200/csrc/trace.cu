@@ -1,15 +1,14 @@
 // trace.cu -- sm_100a kernels of the SBR hot path and the plan that launches them.
 //
-// One work item = a strip of 16x16-ray tiles of one (job, angle) segment.  A CTA
-// (256 threads, one ray per thread, warp = 8x4 ray block) takes items from a
-// device queue (persistent mode) or one item per CTA (per-angle mode), traces the
-// rays through every bounce (trace.cuh) and folds the PO exit-ray term of every
-// frequency of the job into per-thread FP64 sums.  At the end of an item the CTA
-// reduces them in a fixed order and adds the item total, quantised to a per-
-// frequency fixed-point unit, to int64 accumulators with atomicAdd.  Integer
-// addition is associative, so the field is bitwise reproducible whatever order
-// the items finish in (the reference adds FP32 block sums with float atomics,
-// src/cuda/poKernels.cu:118-120, whose order changes run to run).
+// One work item = a run of 8x4-ray blocks of one (job, angle) segment, owned by
+// one warp.  Warps take items from a device queue (persistent grid), trace one
+// 8x4 block of parallel rays at a time through every bounce (trace.cuh), and fold
+// the PO exit-ray term of every frequency of the job into per-lane FP64 sums.  At the end of an item the warp reduces them in
+// a fixed order and adds the total, quantised to a per-frequency fixed-point unit,
+// to int64 accumulators with atomicAdd.  Integer addition is associative, so the
+// field is bitwise reproducible whatever order the items finish in (the reference
+// adds FP32 block sums with float atomics, src/cuda/poKernels.cu:118-120, whose
+// order changes run to run).
 //
 // Replaces launchRaysMultiBounce + integratePoMultiBounce (src/cuda/rtKernels.cu:105-158,
 // src/cuda/poKernels.cu:66-121) and the per-angle loop of runSweep
@@ -33,11 +32,12 @@ struct TraceParams {
     int32_t n_segs;
     int32_t k_begin, k_count;      // frequency sub-range of every job (k_count 0 -> all)
     int32_t count_stats;
+    int32_t n_rep;                 // accumulator replicas per sample
     const JobConst* jobs;
     const FreqConst* freqs;
     int64_t item_begin, item_end;  // items handled by this launch
-    unsigned long long* queue;     // persistent queue head (null -> one item per CTA)
-    unsigned long long* acc;       // [n_samples * 2] fixed-point field accumulators
+    unsigned long long* queue;     // work-queue head of this launch
+    unsigned long long* acc;       // [n_samples][n_rep][2] fixed-point field accumulators
     unsigned long long* acc_stats; // [n_segs * 4]
     uint32_t* err;
     const volatile int32_t* cancel;
@@ -46,130 +46,137 @@ struct TraceParams {
 
 constexpr int kMaxK = 128;   // frequencies per job
 constexpr int kRegK = 4;     // per-lane accumulation up to this many frequencies
+// Resident CTAs (of 4 warps) per SM the kernels are register-budgeted for:
+// 6 -> at most 85 registers per thread, 24 warps per SM.
+constexpr int kMinCtasPerSm = 6;
 
-struct RayOut {
+// State of one ray between closest-hit queries.
+struct RayF {
+    F3 o, d, nl, dl;
+    double L;       // FP64 path (mixed)
+    float dist32;   // FP32 path (reference FP32 arithmetic)
     int count;
-    int queries;
-    float amp;     // 2 cos(theta) R^n, 0 when the ray adds nothing
-    float dist32;  // FP32 path (reference FP32 arithmetic)
-    double L;      // FP64 path
-    float cosT, Rn;
-    double cosD, RnD;  // FP64 copies (SBR_PREC_FP64)
+};
+struct RayD {
+    D3 o, d, nl, dl;
+    double L;
+    int count;
 };
 
-// ------------------------------------------------------------- one ray (FP32/mixed)
-template <int PREC, bool REC>
-__device__ __forceinline__ RayOut trace_ray_f(const SceneView& S, const Segment& G, const JobConst& J, int i, int j,
-                                              uint32_t& err, sbr_ray_record* rec) {
-    F3 o;
-    double L = 0.0;
+// What the PO epilogue needs from a finished ray.
+struct RayOut {
+    float amp;     // 2 cos(theta) R^n, 0 when the ray adds nothing
+    float dist32;
+    double L;
+    float cosT, Rn;
+    double cosD, RnD;
+};
+
+// ------------------------------------------------------------ FP32 / mixed
+template <int PREC>
+__device__ __forceinline__ void start_f(RayF& r, const Segment& G, const JobConst& J, int i, int j) {
     if (PREC == SBR_PREC_FP32) {
-        float u = __fdiv_rn(float(i) + 0.5f, float(J.nx));
-        float v = __fdiv_rn(float(j) + 0.5f, float(J.ny));
-        o = f3(G.llcf[0] + u * G.uf[0] + v * G.vf[0], G.llcf[1] + u * G.uf[1] + v * G.vf[1],
-               G.llcf[2] + u * G.uf[2] + v * G.vf[2]);
+        const float u = __fdiv_rn(float(i) + 0.5f, float(J.nx));
+        const float v = __fdiv_rn(float(j) + 0.5f, float(J.ny));
+        r.o = f3(G.llcf[0] + u * G.uf[0] + v * G.vf[0], G.llcf[1] + u * G.uf[1] + v * G.vf[1],
+                 G.llcf[2] + u * G.uf[2] + v * G.vf[2]);
+        r.L = 0.0;
     } else {
-        double u = (double(i) + 0.5) * J.inv_nx;
-        double v = (double(j) + 0.5) * J.inv_ny;
-        o = f3(float(G.llc[0] + u * G.u[0] + v * G.v[0]), float(G.llc[1] + u * G.u[1] + v * G.v[1]),
-               float(G.llc[2] + u * G.u[2] + v * G.v[2]));
-        L = G.shift;
+        const double u = (double(i) + 0.5) * J.inv_nx;
+        const double v = (double(j) + 0.5) * J.inv_ny;
+        r.o = f3(float(G.llc[0] + u * G.u[0] + v * G.v[0]), float(G.llc[1] + u * G.u[1] + v * G.v[1]),
+                 float(G.llc[2] + u * G.u[2] + v * G.v[2]));
+        r.L = G.shift;
     }
-    F3 d = f3(G.rdf[0], G.rdf[1], G.rdf[2]);
-    float dist32 = 0.0f;
-    int count = 0, queries = 0;
-    F3 nl = f3(0, 0, 0), dl = f3(0, 0, 0);
-    for (int b = 0; b < J.max_bounces; ++b) {
-        float tB = 1e20f;
-        int slot = Walker<false>::closest(S, o, d, 1.0e-3f, tB, err);
-        ++queries;
-        if (slot < 0) break;
-        const GTri* T = S.tris + slot;
-        F3 n = f3(__ldg(&T->p.w), __ldg(&T->e1.w), __ldg(&T->e2.w));
-        nl = n;
-        dl = d;
-        ++count;
-        if (PREC == SBR_PREC_FP32) dist32 += tB;
-        else L += double(tB);
-        if (REC && count <= SBR_MAX_REC) rec->tri[count - 1] = __ldg(S.tri_id + slot);
-        F3 p = o + tB * d;
-        float dn = 2.0f * dot(d, n);
-        d = unit(d - dn * n);
-        o = p + 1.0e-4f * n;
-    }
-    RayOut r;
-    r.count = count;
-    r.queries = queries;
-    r.dist32 = dist32;
-    r.L = (PREC == SBR_PREC_FP32) ? double(dist32) : L;
-    float Rn = 1.0f;
-    for (int b = 0; b < count; ++b) Rn *= J.reflf;
-    float c = dot(nl, f3(-dl.x, -dl.y, -dl.z));
-    r.cosT = c;
-    r.Rn = Rn;
-    r.cosD = c;
-    r.RnD = Rn;
-    r.amp = (count > 0 && c > 0.0f) ? 2.0f * c * Rn : 0.0f;
-    if (REC) {
-        rec->count = count;
-        rec->flags = 1;
-        rec->dist = r.L;
-        rec->normal[0] = nl.x; rec->normal[1] = nl.y; rec->normal[2] = nl.z;
-        rec->lastdir[0] = dl.x; rec->lastdir[1] = dl.y; rec->lastdir[2] = dl.z;
-    }
-    return r;
+    r.d = f3(G.rdf[0], G.rdf[1], G.rdf[2]);
+    r.nl = f3(0, 0, 0);
+    r.dl = f3(0, 0, 0);
+    r.dist32 = 0.0f;
+    r.count = 0;
 }
 
-// ------------------------------------------------------------- one ray (FP64)
+// One closest-hit query, then reflect and nudge; true when the ray is finished.
+template <int PREC, bool REC>
+__device__ __forceinline__ bool step_f(RayF& r, const SceneView& S, int maxB, uint32_t& err, sbr_ray_record* rec) {
+    float tB = 1e20f;
+    const int slot = Walker<false>::closest(S, r.o, r.d, 1.0e-3f, tB, err);
+    if (slot < 0) return true;
+    const GTri* T = S.tris + slot;
+    const F3 n = f3(__ldg(&T->p.w), __ldg(&T->e1.w), __ldg(&T->e2.w));
+    r.nl = n;
+    r.dl = r.d;
+    ++r.count;
+    if (PREC == SBR_PREC_FP32) r.dist32 += tB;
+    else r.L += double(tB);
+    if (REC && r.count <= SBR_MAX_REC) rec->tri[r.count - 1] = __ldg(S.tri_id + slot);
+    const F3 p = r.o + tB * r.d;
+    const float dn = 2.0f * dot(r.d, n);
+    r.d = unit(r.d - dn * n);
+    r.o = p + 1.0e-4f * n;
+    return r.count >= maxB;
+}
+
+template <int PREC>
+__device__ __forceinline__ RayOut finish_f(const RayF& r, const JobConst& J) {
+    RayOut o;
+    float Rn = 1.0f;
+    for (int b = 0; b < r.count; ++b) Rn *= J.reflf;
+    const float c = dot(r.nl, f3(-r.dl.x, -r.dl.y, -r.dl.z));
+    o.cosT = c;
+    o.Rn = Rn;
+    o.cosD = c;
+    o.RnD = Rn;
+    o.dist32 = r.dist32;
+    o.L = (PREC == SBR_PREC_FP32) ? double(r.dist32) : r.L;
+    o.amp = (r.count > 0 && c > 0.0f) ? 2.0f * c * Rn : 0.0f;
+    return o;
+}
+
+// --------------------------------------------------------------------- FP64
+__device__ __forceinline__ void start_d(RayD& r, const Segment& G, const JobConst& J, int i, int j) {
+    const double u = (double(i) + 0.5) / double(J.nx);
+    const double v = (double(j) + 0.5) / double(J.ny);
+    r.o = D3{G.llc[0] + u * G.u[0] + v * G.v[0], G.llc[1] + u * G.u[1] + v * G.v[1],
+             G.llc[2] + u * G.u[2] + v * G.v[2]};
+    r.d = D3{-G.dir[0], -G.dir[1], -G.dir[2]};
+    r.nl = D3{0, 0, 0};
+    r.dl = D3{0, 0, 0};
+    r.L = G.shift;
+    r.count = 0;
+}
+
 template <bool REC>
-__device__ __forceinline__ RayOut trace_ray_d(const SceneView& S, const Segment& G, const JobConst& J, int i, int j,
-                                              uint32_t& err, sbr_ray_record* rec, double& ampD) {
-    double u = (double(i) + 0.5) / double(J.nx);
-    double v = (double(j) + 0.5) / double(J.ny);
-    D3 o{G.llc[0] + u * G.u[0] + v * G.v[0], G.llc[1] + u * G.u[1] + v * G.v[1], G.llc[2] + u * G.u[2] + v * G.v[2]};
-    D3 d{-G.dir[0], -G.dir[1], -G.dir[2]};
-    double L = G.shift;
-    int count = 0, queries = 0;
-    D3 nl{0, 0, 0}, dl{0, 0, 0};
-    for (int b = 0; b < J.max_bounces; ++b) {
-        double tB = 1e20;
-        int slot = Walker<true>::closest(S, o, d, 1.0e-3, tB, err);
-        ++queries;
-        if (slot < 0) break;
-        const GTri64& T = S.tris64[slot];
-        D3 n{T.n[0], T.n[1], T.n[2]};
-        nl = n;
-        dl = d;
-        ++count;
-        L += tB;
-        if (REC && count <= SBR_MAX_REC) rec->tri[count - 1] = __ldg(S.tri_id + slot);
-        D3 p = o + tB * d;
-        double dn = 2.0 * dot(d, n);
-        d = unit(d - dn * n);
-        o = p + 1.0e-4 * n;
-    }
-    RayOut r;
-    r.count = count;
-    r.queries = queries;
-    r.L = L;
-    r.dist32 = float(L);
+__device__ __forceinline__ bool step_d(RayD& r, const SceneView& S, int maxB, uint32_t& err, sbr_ray_record* rec) {
+    double tB = 1e20;
+    const int slot = Walker<true>::closest(S, r.o, r.d, 1.0e-3, tB, err);
+    if (slot < 0) return true;
+    const GTri64& T = S.tris64[slot];
+    const D3 n{T.n[0], T.n[1], T.n[2]};
+    r.nl = n;
+    r.dl = r.d;
+    ++r.count;
+    r.L += tB;
+    if (REC && r.count <= SBR_MAX_REC) rec->tri[r.count - 1] = __ldg(S.tri_id + slot);
+    const D3 p = r.o + tB * r.d;
+    const double dn = 2.0 * dot(r.d, n);
+    r.d = unit(r.d - dn * n);
+    r.o = p + 1.0e-4 * n;
+    return r.count >= maxB;
+}
+
+__device__ __forceinline__ RayOut finish_d(const RayD& r, const JobConst& J) {
+    RayOut o;
     double Rn = 1.0;
-    for (int b = 0; b < count; ++b) Rn *= J.refl;
-    double c = dot(nl, D3{-dl.x, -dl.y, -dl.z});
-    r.cosT = float(c);
-    r.Rn = float(Rn);
-    r.cosD = c;
-    r.RnD = Rn;
-    ampD = (count > 0 && c > 0.0) ? 2.0 * c * Rn : 0.0;
-    r.amp = float(ampD);
-    if (REC) {
-        rec->count = count;
-        rec->flags = 1;
-        rec->dist = L;
-        rec->normal[0] = float(nl.x); rec->normal[1] = float(nl.y); rec->normal[2] = float(nl.z);
-        rec->lastdir[0] = float(dl.x); rec->lastdir[1] = float(dl.y); rec->lastdir[2] = float(dl.z);
-    }
-    return r;
+    for (int b = 0; b < r.count; ++b) Rn *= J.refl;
+    const double c = dot(r.nl, D3{-r.dl.x, -r.dl.y, -r.dl.z});
+    o.cosT = float(c);
+    o.Rn = float(Rn);
+    o.cosD = c;
+    o.RnD = Rn;
+    o.L = r.L;
+    o.dist32 = float(r.L);
+    o.amp = (r.count > 0 && c > 0.0) ? float(2.0 * c * Rn) : 0.0f;
+    return o;
 }
 
 // PO term of one ray at one frequency, added to (re, im).
@@ -177,13 +184,12 @@ __device__ __forceinline__ RayOut trace_ray_d(const SceneView& S, const Segment&
 //  MIXED: phase 2 k L reduced in FP64 by two-constant Cody-Waite, sin/cos of the
 //         reduced FP32 angle, magnitude in FP64.
 //  FP64: the reference USE_DOUBLE arithmetic.
-__device__ __forceinline__ void po_term(int prec, const FreqConst& F, const RayOut& r, double ampD, double& re,
-                                        double& im) {
+__device__ __forceinline__ void po_term(int prec, const FreqConst& F, const RayOut& r, double& re, double& im) {
     if (prec == SBR_PREC_FP32) {
         const float twoPi = 6.28318548202514648438f;
         float phase = (2.0f * F.kf) * r.dist32;
         phase = fmodf(phase, twoPi);
-        float mag = (F.scalef * 2.0f) * r.cosT * r.Rn;
+        const float mag = (F.scalef * 2.0f) * r.cosT * r.Rn;
         float s, c;
         sincosf(phase, &s, &c);
         re += double(-mag * s);
@@ -192,19 +198,19 @@ __device__ __forceinline__ void po_term(int prec, const FreqConst& F, const RayO
         const double twoPiHi = 6.283185307179586232;      // nearest double to 2 pi
         const double twoPiLo = 2.4492935982947064e-16;     // 2 pi - twoPiHi
         const double invTwoPi = 0.15915494309189534561;
-        double ph = 2.0 * F.k * r.L;
-        double q = rint(ph * invTwoPi);
+        const double ph = 2.0 * F.k * r.L;
+        const double q = rint(ph * invTwoPi);
         double red = fma(-q, twoPiHi, ph);
         red = fma(-q, twoPiLo, red);
         float s, c;
         __sincosf(float(red), &s, &c);
-        double mag = F.scale * double(r.amp);
+        const double mag = F.scale * double(r.amp);
         re -= mag * double(s);
         im += mag * double(c);
     } else {
         const double twoPi = 2.0 * 3.14159265358979323846;
-        double phase = fmod((2.0 * F.k) * r.L, twoPi);
-        double mag = (F.scale * 2.0) * r.cosD * r.RnD;
+        const double phase = fmod((2.0 * F.k) * r.L, twoPi);
+        const double mag = (F.scale * 2.0) * r.cosD * r.RnD;
         double s, c;
         sincos(phase, &s, &c);
         re += -mag * s;
@@ -215,7 +221,7 @@ __device__ __forceinline__ void po_term(int prec, const FreqConst& F, const RayO
 __device__ __forceinline__ int find_segment(const int64_t* base, int n, int64_t item) {
     int lo = 0, hi = n;  // base[lo] <= item < base[hi]
     while (hi - lo > 1) {
-        int mid = (lo + hi) >> 1;
+        const int mid = (lo + hi) >> 1;
         if (__ldg(base + mid) <= item) lo = mid;
         else hi = mid;
     }
@@ -223,110 +229,151 @@ __device__ __forceinline__ int find_segment(const int64_t* base, int n, int64_t 
 }
 
 __device__ __forceinline__ void add_fixed(unsigned long long* acc, double v, double invQ) {
-    long long q = __double2ll_rn(v * invQ);
+    const long long q = __double2ll_rn(v * invQ);
     if (q != 0) atomicAdd(acc, (unsigned long long)q);
 }
 
+// Warp-persistent sweep kernel.  Every warp independently takes a work item (a
+// run of 8x4-ray blocks of one (job, angle) segment) and traces it one block at a
+// time, all lanes at the same bounce (no CTA-wide barrier anywhere).  Each lane
+// folds the PO terms of its finished rays into FP64 sums; at the end of the item
+// the warp reduces them in a fixed order and adds the total, as int64 fixed
+// point, to one of the segment's accumulator replicas.  Which lane takes which
+// ray depends only on the item, so every sum is reproducible bit for bit.
 template <int PREC, bool TRANSPOSED, bool REC>
-__global__ void __launch_bounds__(kCtaThreads) k_trace(const TraceParams P) {
-    __shared__ long long s_item;
-    __shared__ int s_seg;
-    __shared__ double2 s_part[kCtaThreads / 32][kMaxK];
-    __shared__ unsigned s_cnt[kCtaThreads / 32][4];
-
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+__global__ void __launch_bounds__(kCtaThreads, kMinCtasPerSm) k_trace(const TraceParams P) {
+    constexpr unsigned FULL = 0xffffffffu;
+    constexpr bool F64 = PREC == SBR_PREC_FP64;
+    constexpr int NACC = TRANSPOSED ? kMaxK / 32 : kRegK;
+    const int lane = threadIdx.x & 31;
+    const int warp_global = (int)((blockIdx.x * (unsigned)kCtaThreads + threadIdx.x) >> 5);
+    const int rep = warp_global % P.n_rep;
     uint32_t err = 0;
     int iter = 0;
     for (;;) {
-        if (threadIdx.x == 0) {
-            long long item;
-            if (P.queue) item = P.item_begin + (long long)atomicAdd(P.queue, 1ull);
-            else item = (iter == 0) ? P.item_begin + blockIdx.x : P.item_end;
+        long long item = 0;
+        if (lane == 0) {
+            item = P.item_begin + (long long)atomicAdd(P.queue, 1ull);
             if (item < P.item_end && P.cancel && (iter & 15) == 0 && *P.cancel != 0) {
                 atomicOr(P.err, DEV_ERR_CANCEL);
                 item = P.item_end;
             }
-            s_item = item;
-            s_seg = item < P.item_end ? find_segment(P.seg_item_base, P.n_segs, item) : -1;
         }
-        __syncthreads();
-        const long long item = s_item;
-        const int seg = s_seg;
-        __syncthreads();
+        item = __shfl_sync(FULL, item, 0);
         if (item >= P.item_end) break;
         ++iter;
 
+        const int seg = find_segment(P.seg_item_base, P.n_segs, item);
         const Segment& G = P.segs[seg];
         const JobConst J = P.jobs[G.job];
         const int kb = P.k_count > 0 ? P.k_begin : 0;
         const int K = P.k_count > 0 ? P.k_count : J.n_freqs;
         const FreqConst* F = P.freqs + J.freq_base + kb;
+        const int b0 = int(item - G.item_base) * G.blocks_per_item;
+        const int nslots = min(G.blocks_per_item, G.blocks - b0) * 32;
+        const int i_end = G.i0 + G.ni, j_end = G.j0 + G.nj;
 
-        double accRe[TRANSPOSED ? kMaxK / 32 : kRegK], accIm[TRANSPOSED ? kMaxK / 32 : kRegK];
+        double accRe[NACC], accIm[NACC];
 #pragma unroll
-        for (int c = 0; c < (TRANSPOSED ? kMaxK / 32 : kRegK); ++c) { accRe[c] = 0.0; accIm[c] = 0.0; }
+        for (int c = 0; c < NACC; ++c) { accRe[c] = 0.0; accIm[c] = 0.0; }
         unsigned cRays = 0, cHit = 0, cBounce = 0, cQuery = 0;
 
-        const long long local = item - G.item_base;
-        const int t0 = int(local) * G.tiles_per_item;
-        const int t1 = min(t0 + G.tiles_per_item, G.tiles);
-        for (int t = t0; t < t1; ++t) {
-            const int tx = t % G.tiles_x, ty = t / G.tiles_x;
-            const int ri = tx * kTileW + (w & 1) * 8 + (lane & 7);
-            const int rj = ty * kTileH + (w >> 1) * 4 + (lane >> 3);
-            const bool valid = ri < G.ni && rj < G.nj;
-            RayOut r;
-            r.count = 0; r.queries = 0; r.amp = 0.0f; r.L = 0.0; r.dist32 = 0.0f; r.cosT = 0.0f; r.Rn = 1.0f;
-            r.cosD = 0.0; r.RnD = 1.0;
-            double ampD = 0.0;
-            if (valid) {
-                const int i = G.i0 + ri, j = G.j0 + rj;
-                sbr_ray_record* rec = nullptr;
-                if (REC) rec = P.records + ((size_t)G.angle * J.nx * J.ny + (size_t)j * J.nx + i);
-                if (PREC == SBR_PREC_FP64) r = trace_ray_d<REC>(P.S, G, J, i, j, err, rec, ampD);
-                else {
-                    r = trace_ray_f<PREC, REC>(P.S, G, J, i, j, err, rec);
-                    ampD = double(r.amp);
+        RayF rf;
+        RayD rd;
+        bool active = false;
+        int queries = 0;
+        sbr_ray_record* rec = nullptr;
+        int next = 0;  // next slot of the item to hand out (same value in every lane)
+
+        auto refill = [&]() {
+            for (;;) {
+                const unsigned need = __ballot_sync(FULL, !active);
+                if (need == 0 || next >= nslots) break;
+                const int s = next + __popc(need & ((1u << lane) - 1u));
+                if (!active && s < nslots) {
+                    const int blk = b0 + (s >> 5), l = s & 31;
+                    const int i = G.i0 + (blk % G.blocks_x) * kBlockW + (l & 7);
+                    const int j = G.j0 + (blk / G.blocks_x) * kBlockH + (l >> 3);
+                    if (i < i_end && j < j_end) {
+                        if (F64) start_d(rd, G, J, i, j);
+                        else start_f<PREC>(rf, G, J, i, j);
+                        active = true;
+                        queries = 0;
+                        ++cRays;
+                        if (REC) rec = P.records + ((size_t)G.angle * J.nx * J.ny + (size_t)j * J.nx + i);
+                    }
                 }
-                cRays += 1;
-                cHit += r.count > 0;
-                cBounce += r.count;
-                cQuery += r.queries;
+                next += __popc(need);
+            }
+        };
+
+        refill();
+        while (__any_sync(FULL, active)) {
+            bool done = false;
+            RayOut out;
+            out.amp = 0.0f;
+            if (active) {
+                done = F64 ? step_d<REC>(rd, P.S, J.max_bounces, err, rec)
+                           : step_f<PREC, REC>(rf, P.S, J.max_bounces, err, rec);
+                ++queries;
+                if (done) {
+                    const int cnt = F64 ? rd.count : rf.count;
+                    out = F64 ? finish_d(rd, J) : finish_f<PREC>(rf, J);
+                    cHit += cnt > 0;
+                    cBounce += cnt;
+                    cQuery += queries;
+                    active = false;
+                    if (REC) {
+                        rec->count = cnt;
+                        rec->flags = 1;
+                        rec->dist = out.L;
+                        if (F64) {
+                            rec->normal[0] = float(rd.nl.x); rec->normal[1] = float(rd.nl.y); rec->normal[2] = float(rd.nl.z);
+                            rec->lastdir[0] = float(rd.dl.x); rec->lastdir[1] = float(rd.dl.y); rec->lastdir[2] = float(rd.dl.z);
+                        } else {
+                            rec->normal[0] = rf.nl.x; rec->normal[1] = rf.nl.y; rec->normal[2] = rf.nl.z;
+                            rec->lastdir[0] = rf.dl.x; rec->lastdir[1] = rf.dl.y; rec->lastdir[2] = rf.dl.z;
+                        }
+                    }
+                }
             }
             if (!TRANSPOSED) {
-                if (r.amp != 0.0f) {
+                if (done && out.amp != 0.0f) {
 #pragma unroll
                     for (int k = 0; k < kRegK; ++k)
-                        if (k < K) po_term(PREC, F[k], r, ampD, accRe[k], accIm[k]);
+                        if (k < K) po_term(PREC, F[k], out, accRe[k], accIm[k]);
                 }
             } else {
-                // every lane owns frequencies lane, lane + 32, ...; rays are visited
-                // in lane order so the per-frequency sum order is fixed
-                unsigned m = __ballot_sync(0xffffffffu, r.amp != 0.0f);
+                // lanes own frequencies lane, lane + 32, ...; finished rays are taken
+                // in lane order, so every frequency's sum has a fixed order
+                unsigned m = __ballot_sync(FULL, done && out.amp != 0.0f);
                 while (m) {
                     const int src = __ffs(m) - 1;
                     m &= m - 1;
                     RayOut q;
-                    q.amp = __shfl_sync(0xffffffffu, r.amp, src);
-                    q.L = __shfl_sync(0xffffffffu, r.L, src);
-                    q.dist32 = __shfl_sync(0xffffffffu, r.dist32, src);
-                    q.cosT = __shfl_sync(0xffffffffu, r.cosT, src);
-                    q.Rn = __shfl_sync(0xffffffffu, r.Rn, src);
-                    if (PREC == SBR_PREC_FP64) {
-                        q.cosD = __shfl_sync(0xffffffffu, r.cosD, src);
-                        q.RnD = __shfl_sync(0xffffffffu, r.RnD, src);
-                    }
-                    double qa = __shfl_sync(0xffffffffu, ampD, src);
+                    q.amp = __shfl_sync(FULL, out.amp, src);
+                    q.L = __shfl_sync(FULL, out.L, src);
+                    q.dist32 = __shfl_sync(FULL, out.dist32, src);
+                    q.cosT = __shfl_sync(FULL, out.cosT, src);
+                    q.Rn = __shfl_sync(FULL, out.Rn, src);
+                    q.cosD = F64 ? __shfl_sync(FULL, out.cosD, src) : 0.0;
+                    q.RnD = F64 ? __shfl_sync(FULL, out.RnD, src) : 0.0;
 #pragma unroll
-                    for (int c = 0; c < kMaxK / 32; ++c) {
+                    for (int c = 0; c < NACC; ++c) {
                         const int k = c * 32 + lane;
-                        if (k < K) po_term(PREC, F[k], q, qa, accRe[c], accIm[c]);
+                        if (k < K) po_term(PREC, F[k], q, accRe[c], accIm[c]);
                     }
                 }
             }
+            // the next 8x4 block starts when the whole warp is done with this one:
+            // keeping the warp's rays at the same bounce keeps them coherent (they
+            // share direction and walk the same nodes), which is worth more than
+            // refilling idle lanes
+            if (!__any_sync(FULL, active)) refill();
         }
 
-        // ---- fold the item: lanes -> warp -> CTA in a fixed order
+        // ---- fold the item: lanes -> warp in a fixed order, then fixed point
+        const long long sbase = G.sample_base + kb;
         if (!TRANSPOSED) {
 #pragma unroll
             for (int k = 0; k < kRegK; ++k) {
@@ -334,71 +381,71 @@ __global__ void __launch_bounds__(kCtaThreads) k_trace(const TraceParams P) {
                     double a = accRe[k], b = accIm[k];
 #pragma unroll
                     for (int off = 16; off > 0; off >>= 1) {
-                        a += __shfl_xor_sync(0xffffffffu, a, off);
-                        b += __shfl_xor_sync(0xffffffffu, b, off);
+                        a += __shfl_xor_sync(FULL, a, off);
+                        b += __shfl_xor_sync(FULL, b, off);
                     }
-                    if (lane == 0) s_part[w][k] = make_double2(a, b);
+                    if (lane == k) {
+                        unsigned long long* A = P.acc + 2 * ((sbase + k) * P.n_rep + rep);
+                        add_fixed(A, a, F[k].inv_quantum);
+                        add_fixed(A + 1, b, F[k].inv_quantum);
+                    }
                 }
             }
         } else {
 #pragma unroll
-            for (int c = 0; c < kMaxK / 32; ++c) {
+            for (int c = 0; c < NACC; ++c) {
                 const int k = c * 32 + lane;
-                if (k < K) s_part[w][k] = make_double2(accRe[c], accIm[c]);
+                if (k < K) {
+                    unsigned long long* A = P.acc + 2 * ((sbase + k) * P.n_rep + rep);
+                    add_fixed(A, accRe[c], F[k].inv_quantum);
+                    add_fixed(A + 1, accIm[c], F[k].inv_quantum);
+                }
             }
         }
-        cRays = __reduce_add_sync(0xffffffffu, cRays);
-        cHit = __reduce_add_sync(0xffffffffu, cHit);
-        cBounce = __reduce_add_sync(0xffffffffu, cBounce);
-        cQuery = __reduce_add_sync(0xffffffffu, cQuery);
-        if (lane == 0) {
-            s_cnt[w][0] = cRays; s_cnt[w][1] = cHit; s_cnt[w][2] = cBounce; s_cnt[w][3] = cQuery;
-        }
-        __syncthreads();
-        if (threadIdx.x < K) {
-            const int k = threadIdx.x;
-            double a = 0.0, b = 0.0;
-#pragma unroll
-            for (int ww = 0; ww < kCtaThreads / 32; ++ww) { a += s_part[ww][k].x; b += s_part[ww][k].y; }
-            const long long s = G.sample_base + kb + k;
-            const double iq = F[k].inv_quantum;
-            add_fixed(P.acc + 2 * s, a, iq);
-            add_fixed(P.acc + 2 * s + 1, b, iq);
-        }
-        if (P.count_stats && threadIdx.x >= 128 && threadIdx.x < 132) {
-            const int c = threadIdx.x - 128;
-            unsigned long long tot = 0;
-#pragma unroll
-            for (int ww = 0; ww < kCtaThreads / 32; ++ww) tot += s_cnt[ww][c];
-            if (tot) atomicAdd(P.acc_stats + 4 * (size_t)seg + c, tot);
+        if (P.count_stats) {
+            cRays = __reduce_add_sync(FULL, cRays);
+            cHit = __reduce_add_sync(FULL, cHit);
+            cBounce = __reduce_add_sync(FULL, cBounce);
+            cQuery = __reduce_add_sync(FULL, cQuery);
+            if (lane < 4) {
+                const unsigned v = lane == 0 ? cRays : lane == 1 ? cHit : lane == 2 ? cBounce : cQuery;
+                if (v) atomicAdd(P.acc_stats + 4 * (size_t)seg + lane, (unsigned long long)v);
+            }
         }
     }
     if (err) atomicOr(P.err, err);
 }
 
-// Converts the fixed-point accumulators to fields and clears them (and the
-// queue) so the plan can run again without a memset.
-__global__ void k_finalize(long long n_samples, const double* __restrict__ quantum, unsigned long long* acc,
-                           double* field, long long n_stats, unsigned long long* acc_stats,
-                           unsigned long long* out_stats, unsigned long long* queue) {
-    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+// Converts the fixed-point accumulators (summing the replicas exactly, as
+// integers) to fields, copies the counters, and clears accumulators, counters
+// and queue heads so the plan can run again without a memset.
+__global__ void k_finalize(long long n_samples, int n_rep, const double* __restrict__ quantum,
+                           unsigned long long* acc, double* field, long long n_stats,
+                           unsigned long long* acc_stats, unsigned long long* out_stats, unsigned long long* queue,
+                           long long n_queue) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t < n_samples) {
-        double q = quantum[t];
-        long long re = (long long)acc[2 * t], im = (long long)acc[2 * t + 1];
+        long long re = 0, im = 0;
+        for (int r = 0; r < n_rep; ++r) {
+            unsigned long long* A = acc + 2 * (t * n_rep + r);
+            re += (long long)A[0];
+            im += (long long)A[1];
+            A[0] = 0ull;
+            A[1] = 0ull;
+        }
+        const double q = quantum[t];
         field[2 * t] = double(re) * q;
         field[2 * t + 1] = double(im) * q;
-        acc[2 * t] = 0ull;
-        acc[2 * t + 1] = 0ull;
     }
     if (t < n_stats) {
         out_stats[t] = acc_stats[t];
         acc_stats[t] = 0ull;
     }
-    if (t == 0) *queue = 0ull;
+    if (t < n_queue) queue[t] = 0ull;
 }
 
 __global__ void k_fill_records(sbr_ray_record* r, long long n) {
-    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= n) return;
     sbr_ray_record z;
     z.count = 0;
@@ -437,6 +484,21 @@ sbr_status launch_trace(const void* fn, int grid, cudaStream_t st, const TracePa
     return SBR_OK;
 }
 
+sbr_status resident_ctas(const void* fn, int ctas_per_sm, int num_sms, int* out) {
+    int occ = 0;
+    SBR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kCtaThreads, 0));
+    *out = std::max(1, ctas_per_sm > 0 ? ctas_per_sm : occ) * num_sms;
+    return SBR_OK;
+}
+
+void finalize(long long n_samples, int n_rep, const double* quantum, unsigned long long* acc, double* field,
+              long long n_stats, unsigned long long* acc_stats, unsigned long long* out_stats,
+              unsigned long long* queue, long long n_queue, cudaStream_t st) {
+    long long nmax = std::max(std::max(n_samples, n_stats), std::max(n_queue, 1LL));
+    k_finalize<<<(unsigned)((nmax + 255) / 256), 256, 0, st>>>(n_samples, n_rep, quantum, acc, field, n_stats,
+                                                               acc_stats, out_stats, queue, n_queue);
+}
+
 }  // namespace
 
 sbr_status plan_launch(sbr_plan* pl, bool records, sbr_ray_record* d_records) {
@@ -447,6 +509,7 @@ sbr_status plan_launch(sbr_plan* pl, bool records, sbr_ray_record* d_records) {
     p.segs = pl->d_segs;
     p.seg_item_base = pl->d_seg_base;
     p.n_segs = (int32_t)pl->n_segs;
+    p.n_rep = kAccReplicas;
     p.jobs = pl->d_jobs;
     p.freqs = pl->d_freqs;
     p.acc = pl->d_acc;
@@ -457,29 +520,28 @@ sbr_status plan_launch(sbr_plan* pl, bool records, sbr_ray_record* d_records) {
     cudaStream_t st = pl->stream;
     int launches = 0;
     if (pl->n_items > 0) {
+        if (pl->persistent_grid <= 0) {
+            sbr_status s = resident_ctas(fn, pl->ctas_per_sm, pl->num_sms, &pl->persistent_grid);
+            if (s != SBR_OK) return s;
+        }
         if (pl->mode == SBR_MODE_BATCHED || records) {
-            if (pl->persistent_grid <= 0) {
-                int occ = 0;
-                SBR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kCtaThreads, 0));
-                int per = pl->ctas_per_sm > 0 ? pl->ctas_per_sm : std::max(1, occ);
-                pl->persistent_grid = std::max(1, per * pl->num_sms);
-            }
             p.k_begin = 0;
             p.k_count = 0;
             p.count_stats = 1;
             p.item_begin = 0;
             p.item_end = pl->n_items;
             p.queue = pl->d_queue;
-            int grid = (int)std::min<long long>(pl->persistent_grid, pl->n_items);
+            const long long warps_needed = pl->n_items;
+            const int grid = (int)std::min<long long>(pl->persistent_grid, (warps_needed + 3) / 4);
             sbr_status s = launch_trace(fn, grid, st, p);
             if (s != SBR_OK) return s;
             ++launches;
         } else {
-            // the reference loop: one trace + PO launch per (angle, frequency)
-            p.queue = nullptr;
+            // the reference loop: one trace + PO launch per (angle, frequency), each
+            // with its own queue head
             for (size_t g = 0; g < pl->segs.size(); ++g) {
                 const Segment& G = pl->segs[g];
-                long long n = pl->seg_base[g + 1] - pl->seg_base[g];
+                const long long n = pl->seg_base[g + 1] - pl->seg_base[g];
                 if (n == 0) continue;
                 const JobConst& J = pl->jobs[G.job];
                 for (int k = 0; k < J.n_freqs; ++k) {
@@ -488,18 +550,17 @@ sbr_status plan_launch(sbr_plan* pl, bool records, sbr_ray_record* d_records) {
                     p.count_stats = k == 0;
                     p.item_begin = pl->seg_base[g];
                     p.item_end = pl->seg_base[g + 1];
-                    sbr_status s = launch_trace(fn, (int)n, st, p);
+                    p.queue = pl->d_queue + 1 + G.sample_base + k;
+                    const int grid = (int)std::min<long long>(pl->persistent_grid, (n + 3) / 4);
+                    sbr_status s = launch_trace(fn, grid, st, p);
                     if (s != SBR_OK) return s;
                     ++launches;
                 }
             }
         }
     }
-    long long nmax = std::max<long long>(pl->n_samples, (long long)pl->n_segs * 4);
-    nmax = std::max<long long>(nmax, 1);
-    int blocks = (int)((nmax + 255) / 256);
-    k_finalize<<<blocks, 256, 0, st>>>(pl->n_samples, pl->d_quantum, pl->d_acc, pl->d_field,
-                                       (long long)pl->n_segs * 4, pl->d_acc_stats, pl->d_stats, pl->d_queue);
+    finalize(pl->n_samples, kAccReplicas, pl->d_quantum, pl->d_acc, pl->d_field, (long long)pl->n_segs * 4,
+             pl->d_acc_stats, pl->d_stats, pl->d_queue, pl->n_samples + 1, st);
     SBR_CUDA(cudaGetLastError());
     ++launches;
     pl->launches = launches;
@@ -644,9 +705,9 @@ extern "C" sbr_status sbr_run_noalloc(sbr_scene* s, const sbr_job* job, double* 
 
     if (tot.n_items > 0) {
         const void* fn = pick_kernel(o.precision, tot.k_max > kRegK, false);
-        int occ = 0;
-        SBR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kCtaThreads, 0));
-        int per = o.ctas_per_sm > 0 ? o.ctas_per_sm : std::max(1, occ);
+        int resident = 0;
+        st = resident_ctas(fn, o.ctas_per_sm, s->num_sms, &resident);
+        if (st != SBR_OK) return st;
         TraceParams p{};
         p.S = s->view();
         p.segs = D->tables.segs;
@@ -655,6 +716,7 @@ extern "C" sbr_status sbr_run_noalloc(sbr_scene* s, const sbr_job* job, double* 
         p.k_begin = 0;
         p.k_count = 0;
         p.count_stats = 1;
+        p.n_rep = 1;
         p.jobs = &D->tables.job;
         p.freqs = D->tables.freqs;
         p.item_begin = 0;
@@ -665,14 +727,12 @@ extern "C" sbr_status sbr_run_noalloc(sbr_scene* s, const sbr_job* job, double* 
         p.err = s->d_err;
         p.cancel = s->d_cancel;
         p.records = nullptr;
-        int grid = (int)std::min<long long>((long long)per * s->num_sms, tot.n_items);
+        const int grid = (int)std::min<long long>(resident, (tot.n_items + 3) / 4);
         st = launch_trace(fn, grid, stream, p);
         if (st != SBR_OK) return st;
     }
-    long long nmax = std::max<long long>(std::max<long long>((long long)nsamp, 4LL * (long long)nseg), 1);
-    k_finalize<<<(unsigned)((nmax + 255) / 256), 256, 0, stream>>>(
-        (long long)nsamp, D->tables.quantum, D->acc, d_field, d_stats ? 4LL * (long long)nseg : 0LL, D->acc_stats,
-        reinterpret_cast<unsigned long long*>(d_stats), &D->queue);
+    finalize((long long)nsamp, 1, D->tables.quantum, D->acc, d_field, d_stats ? 4LL * (long long)nseg : 0LL,
+             D->acc_stats, reinterpret_cast<unsigned long long*>(d_stats), &D->queue, 1, stream);
     SBR_CUDA(cudaGetLastError());
     SBR_CUDA(cudaStreamSynchronize(stream));
 

@@ -35,9 +35,11 @@ __device__ __forceinline__ float dot(F3 a, F3 b) { return a.x * b.x + a.y * b.y 
 __device__ __forceinline__ F3 cross(F3 a, F3 b) {
     return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
 }
+// Normalisation with the hardware reciprocal square root (a few ulp, like the
+// reference's --use_fast_math FP32 build).
 __device__ __forceinline__ F3 unit(F3 a) {
-    float l = sqrtf(a.x * a.x + a.y * a.y + a.z * a.z);
-    return {__fdiv_rn(a.x, l), __fdiv_rn(a.y, l), __fdiv_rn(a.z, l)};
+    float r = rsqrtf(a.x * a.x + a.y * a.y + a.z * a.z);
+    return {a.x * r, a.y * r, a.z * r};
 }
 __device__ __forceinline__ D3 operator+(D3 a, D3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
 __device__ __forceinline__ D3 operator-(D3 a, D3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
@@ -51,27 +53,43 @@ __device__ __forceinline__ D3 unit(D3 a) {
     return {a.x / l, a.y / l, a.z / l};
 }
 
-// Per-thread traversal counters.
-struct QueryCount {
-    uint32_t iters;
-};
-
-__device__ __forceinline__ float safe_inv(float d) {
-    return __frcp_rn(fabsf(d) > 1e-20f ? d : copysignf(1e-20f, d));
+// Three-input min / max (sm_100 PTX); like fminf/fmaxf they return the other
+// operand when one is NaN.
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
 }
-__device__ __forceinline__ double safe_inv(double d) { return 1.0 / (fabs(d) > 1e-200 ? d : copysign(1e-200, d)); }
+__device__ __forceinline__ float min3f(float a, float b, float c) {
+    float d;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
 
-// Slab entry distance of one child box, +inf when missed.  Boxes are stored
-// conservatively; the exit is widened by a relative 2^-20 so rounding of the
-// FMA form never rejects a box the ray touches.
+// Reciprocal direction for the slab tests.  Components below 1e-20 in magnitude
+// are clamped (keeps the slab arithmetic finite, no 0 * inf); the approximate
+// reciprocal's relative error (< 2^-22) is covered by the slab slack below.
+__device__ __forceinline__ float slab_inv(float d) {
+    float c = fabsf(d) > 1e-20f ? d : copysignf(1e-20f, d);
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(c));
+    return r;
+}
+__device__ __forceinline__ double slab_inv(double d) { return 1.0 / (fabs(d) > 1e-200 ? d : copysign(1e-200, d)); }
+
+// Entry distance of a box, +inf when missed.  Boxes are conservative; the exit is
+// widened by a relative 2^-20 so neither the FMA form nor the approximate
+// reciprocal ever rejects a box the ray touches (boxes only prune, the triangle
+// test decides every hit).
+constexpr float kSlabSlack = 1.00000095367431640625f;  // 1 + 2^-20
 __device__ __forceinline__ float slab_f(float lx, float hx, float ly, float hy, float lz, float hz, F3 inv, F3 oi,
                                         float tMin, float tMax) {
     float x0 = fmaf(lx, inv.x, -oi.x), x1 = fmaf(hx, inv.x, -oi.x);
     float y0 = fmaf(ly, inv.y, -oi.y), y1 = fmaf(hy, inv.y, -oi.y);
     float z0 = fmaf(lz, inv.z, -oi.z), z1 = fmaf(hz, inv.z, -oi.z);
-    float tn = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), tMin));
-    float tf = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), tMax));
-    return tn <= tf * 1.00000095367431640625f ? tn : __int_as_float(0x7f800000);
+    float tn = max3f(fminf(x0, x1), fminf(y0, y1), fmaxf(fminf(z0, z1), tMin));
+    float tf = min3f(fmaxf(x0, x1), fmaxf(y0, y1), fminf(fmaxf(z0, z1), tMax));
+    return tn <= tf * kSlabSlack ? tn : __int_as_float(0x7f800000);
 }
 __device__ __forceinline__ double slab_d(double lx, double hx, double ly, double hy, double lz, double hz, D3 o,
                                          D3 inv, double tMin, double tMax) {
@@ -83,7 +101,7 @@ __device__ __forceinline__ double slab_d(double lx, double hx, double ly, double
     return tn <= tf * (1.0 + 1e-12) ? tn : __longlong_as_double(0x7ff0000000000000LL);
 }
 
-// Moller-Trumbore in the reference's operation order (FP32).
+// Moller-Trumbore in the reference's operation order.
 __device__ __forceinline__ bool mt_f(const GTri& T, F3 o, F3 d, float tMin, float tMax, float& t) {
     F3 e1 = f3(T.e1.x, T.e1.y, T.e1.z), e2 = f3(T.e2.x, T.e2.y, T.e2.z);
     F3 pv = cross(d, e2);
@@ -131,8 +149,17 @@ __device__ __forceinline__ GNode load_node(const GNode* p) {
 
 constexpr uint32_t kIterBudget = 1u << 22;  // node + leaf steps per query before giving up
 
-// Closest hit along o + t d, t in [tMin, tBest].  Returns the leaf slot of the hit
-// triangle (or -1).  `err` collects DEV_ERR_* bits.
+// Stack entry: child reference in the low word, entry distance (float bits, or the
+// FP64 distance rounded down to float) in the high word.
+__device__ __forceinline__ unsigned long long pack_entry(int ref, float t) {
+    return ((unsigned long long)__float_as_uint(t) << 32) | (unsigned)ref;
+}
+
+// Closest hit along o + t d with t in [tMin, tBest]: returns the leaf slot of the hit
+// triangle (or -1) and lowers tBest to its distance.  While-while structure:
+// inner nodes are walked (nearer child first, farther child pushed with its entry
+// distance) until a leaf is reached, leaves are tested, popped entries beyond the
+// current hit are skipped.  `err` collects DEV_ERR_* bits.
 template <bool kF64>
 struct Walker;
 
@@ -140,48 +167,51 @@ template <>
 struct Walker<false> {
     __device__ __forceinline__ static int closest(const SceneView& S, F3 o, F3 d, float tMin, float& tBest,
                                                   uint32_t& err) {
-        F3 inv{safe_inv(d.x), safe_inv(d.y), safe_inv(d.z)};
-        F3 oi{o.x * inv.x, o.y * inv.y, o.z * inv.z};
-        int stRef[kStackDepth];
-        float stT[kStackDepth];
+        const F3 inv{slab_inv(d.x), slab_inv(d.y), slab_inv(d.z)};
+        const F3 oi{o.x * inv.x, o.y * inv.y, o.z * inv.z};
+        unsigned long long stack[kStackDepth];
         int sp = 0;
         int ref = 0;
         int best = -1;
         uint32_t iters = 0;
-        while (true) {
-            if (++iters > kIterBudget) { err |= DEV_ERR_BUDGET; return -1; }
-            if (ref >= 0) {
-                GNode n = load_node(S.nodes + ref);
-                float t0 = slab_f(n.a.x, n.a.y, n.a.z, n.a.w, n.c.x, n.c.y, inv, oi, tMin, tBest);
-                float t1 = slab_f(n.b.x, n.b.y, n.b.z, n.b.w, n.c.z, n.c.w, inv, oi, tMin, tBest);
-                bool h0 = t0 <= tBest, h1 = t1 <= tBest;
+        for (;;) {
+            while (ref >= 0) {
+                if (++iters > kIterBudget) { err |= DEV_ERR_BUDGET; return -1; }
+                const GNode n = load_node(S.nodes + ref);
+                const float t0 = slab_f(n.a.x, n.a.y, n.a.z, n.a.w, n.c.x, n.c.y, inv, oi, tMin, tBest);
+                const float t1 = slab_f(n.b.x, n.b.y, n.b.z, n.b.w, n.c.z, n.c.w, inv, oi, tMin, tBest);
+                const bool h0 = t0 <= tBest, h1 = t1 <= tBest;
                 if (h0 && h1) {
-                    bool f = t1 < t0;
-                    int nearRef = f ? n.link.y : n.link.x;
-                    int farRef = f ? n.link.x : n.link.y;
-                    float farT = f ? t0 : t1;
-                    if (sp < kStackDepth) { stRef[sp] = farRef; stT[sp] = farT; ++sp; }
+                    const bool f = t1 < t0;
+                    if (sp < kStackDepth) stack[sp++] = pack_entry(f ? n.link.x : n.link.y, f ? t0 : t1);
                     else err |= DEV_ERR_STACK;
-                    ref = nearRef;
-                    continue;
+                    ref = f ? n.link.y : n.link.x;
+                } else if (h0 || h1) {
+                    ref = h0 ? n.link.x : n.link.y;
+                } else {
+                    bool found = false;
+                    while (sp > 0) {
+                        const unsigned long long e = stack[--sp];
+                        if (__uint_as_float((unsigned)(e >> 32)) <= tBest) { ref = (int)(unsigned)e; found = true; break; }
+                    }
+                    if (!found) return best;
                 }
-                if (h0) { ref = n.link.x; continue; }
-                if (h1) { ref = n.link.y; continue; }
-            } else {
-                int code = ~ref;
-                int first = code >> 4, cnt = code & 15;
+            }
+            do {
+                if (++iters > kIterBudget) { err |= DEV_ERR_BUDGET; return -1; }
+                const int code = ~ref;
+                const int first = code >> 4, cnt = code & 15;
                 for (int k = 0; k < cnt; ++k) {
                     float t;
                     if (mt_f(S.tris[first + k], o, d, tMin, tBest, t)) { tBest = t; best = first + k; }
                 }
-            }
-            // pop the next entry that can still hold a closer hit
-            bool found = false;
-            while (sp > 0) {
-                --sp;
-                if (stT[sp] <= tBest) { ref = stRef[sp]; found = true; break; }
-            }
-            if (!found) return best;
+                bool found = false;
+                while (sp > 0) {
+                    const unsigned long long e = stack[--sp];
+                    if (__uint_as_float((unsigned)(e >> 32)) <= tBest) { ref = (int)(unsigned)e; found = true; break; }
+                }
+                if (!found) return best;
+            } while (ref < 0);
         }
     }
 };
@@ -190,46 +220,53 @@ template <>
 struct Walker<true> {
     __device__ __forceinline__ static int closest(const SceneView& S, D3 o, D3 d, double tMin, double& tBest,
                                                   uint32_t& err) {
-        D3 inv{safe_inv(d.x), safe_inv(d.y), safe_inv(d.z)};
-        int stRef[kStackDepth];
-        double stT[kStackDepth];
+        const D3 inv{slab_inv(d.x), slab_inv(d.y), slab_inv(d.z)};
+        unsigned long long stack[kStackDepth];
         int sp = 0;
         int ref = 0;
         int best = -1;
         uint32_t iters = 0;
-        while (true) {
-            if (++iters > kIterBudget) { err |= DEV_ERR_BUDGET; return -1; }
-            if (ref >= 0) {
-                GNode n = load_node(S.nodes + ref);
-                double t0 = slab_d(n.a.x, n.a.y, n.a.z, n.a.w, n.c.x, n.c.y, o, inv, tMin, tBest);
-                double t1 = slab_d(n.b.x, n.b.y, n.b.z, n.b.w, n.c.z, n.c.w, o, inv, tMin, tBest);
-                bool h0 = t0 <= tBest, h1 = t1 <= tBest;
+        // entry distances are stored rounded down to float, so the pruning test
+        // (entry <= tBest) stays conservative
+        auto down = [](double t) { return __double2float_rd(t); };
+        for (;;) {
+            while (ref >= 0) {
+                if (++iters > kIterBudget) { err |= DEV_ERR_BUDGET; return -1; }
+                const GNode n = load_node(S.nodes + ref);
+                const double t0 = slab_d(n.a.x, n.a.y, n.a.z, n.a.w, n.c.x, n.c.y, o, inv, tMin, tBest);
+                const double t1 = slab_d(n.b.x, n.b.y, n.b.z, n.b.w, n.c.z, n.c.w, o, inv, tMin, tBest);
+                const bool h0 = t0 <= tBest, h1 = t1 <= tBest;
                 if (h0 && h1) {
-                    bool f = t1 < t0;
-                    int nearRef = f ? n.link.y : n.link.x;
-                    int farRef = f ? n.link.x : n.link.y;
-                    double farT = f ? t0 : t1;
-                    if (sp < kStackDepth) { stRef[sp] = farRef; stT[sp] = farT; ++sp; }
+                    const bool f = t1 < t0;
+                    if (sp < kStackDepth) stack[sp++] = pack_entry(f ? n.link.x : n.link.y, down(f ? t0 : t1));
                     else err |= DEV_ERR_STACK;
-                    ref = nearRef;
-                    continue;
+                    ref = f ? n.link.y : n.link.x;
+                } else if (h0 || h1) {
+                    ref = h0 ? n.link.x : n.link.y;
+                } else {
+                    bool found = false;
+                    while (sp > 0) {
+                        const unsigned long long e = stack[--sp];
+                        if (double(__uint_as_float((unsigned)(e >> 32))) <= tBest) { ref = (int)(unsigned)e; found = true; break; }
+                    }
+                    if (!found) return best;
                 }
-                if (h0) { ref = n.link.x; continue; }
-                if (h1) { ref = n.link.y; continue; }
-            } else {
-                int code = ~ref;
-                int first = code >> 4, cnt = code & 15;
+            }
+            do {
+                if (++iters > kIterBudget) { err |= DEV_ERR_BUDGET; return -1; }
+                const int code = ~ref;
+                const int first = code >> 4, cnt = code & 15;
                 for (int k = 0; k < cnt; ++k) {
                     double t;
                     if (mt_d(S.tris64[first + k], o, d, tMin, tBest, t)) { tBest = t; best = first + k; }
                 }
-            }
-            bool found = false;
-            while (sp > 0) {
-                --sp;
-                if (stT[sp] <= tBest) { ref = stRef[sp]; found = true; break; }
-            }
-            if (!found) return best;
+                bool found = false;
+                while (sp > 0) {
+                    const unsigned long long e = stack[--sp];
+                    if (double(__uint_as_float((unsigned)(e >> 32))) <= tBest) { ref = (int)(unsigned)e; found = true; break; }
+                }
+                if (!found) return best;
+            } while (ref < 0);
         }
     }
 };
