@@ -1,25 +1,34 @@
 """Benchmark of the SBR hot path on B200: angle-frequency samples/s and Mray-bounces/s.
 
-Workload (default, one GPU): square trihedral corner reflector, 1 m edges, 3 x
-100x100x2 = 60,000 triangles, 10 GHz, 10 rays/lambda over the bounding aperture
-(G = sqrt(3) m, 578 x 578 = 334,084 rays per angle), max 3 bounces, 2-D sweep
-theta = 0..90 x phi = 0..90 deg at 1 deg (8,281 angles), all drained by one
-persistent launch.  Synthetic, seeded mesh (no dataset is involved).
+Default workload (the metric's one-GPU configuration): square trihedral corner
+reflector, 1 m edges, 3 x 100x100x2 = 60,000 triangles, 10 GHz, 10 rays/lambda over
+the bounding aperture (G = sqrt(3) m, 578 x 578 = 334,084 rays per angle), max 3
+bounces, 2-D sweep theta = 0..90 x phi = 0..90 deg at 1 deg (8,281 angles), all
+drained by one persistent launch.  Other workloads (--workload): `sphere` (icosphere
+level 5, 1 GHz, 67^2 rays, 3 bounces, 360 azimuths), `aircraft` (seeded ~2.15 M
+triangle aircraft, 64 frequencies log-spaced over 1-18 GHz, 721 azimuths at 0.5 deg,
+5 bounces) and `aircraft-dev` (8 frequencies x 73 azimuths of the same).  All meshes
+are synthetic and seeded; no dataset is involved.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
 
-`value`      whole-job samples/s with the plan resident in HBM (sbr_plan_execute on
-             torch's current stream, CUDA events, L2 flushed between steps).
-`e2e`        the same metric through sbr_run with host arrays in and out (frames,
-             item table H2D, fields D2H inside the timed region).
-`roofline`   dominant kernel (k_trace): algorithmic FP32 work per closest-hit
-             query on the reference SAH tree, 27 V_box + 57 V_tri FLOP, with
-             V_box / V_tri counted by the instrumented CPU oracle on a sample of the
-             same sweep; peak = FP32 SGEMM throughput measured here (the driver's
-             peak file has HBM and bf16 only).
+`value`      whole-job samples/s of the batched engine with the plan resident in HBM
+             (sbr_plan_execute on a torch stream, CUDA events, L2 flushed by a 256 MiB
+             write before every step, inside the timed region).  All frequencies of a
+             workload share one trace on the grid of the highest frequency.
+`e2e`        the same metric through sbr_run with host arrays in and out.
+`per_angle`  the reference's loop structure: one trace + PO launch per (angle,
+             frequency), each frequency on its own grid n_f = ceil(10 G f / c), FP32
+             arithmetic (the baseline of the >= 10x target), on a subset of angles.
+`fp64_check` batched mixed precision against a full-FP64 run of the same batched job.
+`roofline`   dominant kernel (k_trace): algorithmic FP32 work per closest-hit query
+             on the reference SAH tree, 27 V_box + 57 V_tri FLOP, V_box / V_tri counted
+             by the instrumented CPU oracle on a sample of the same sweep; peak = FP32
+             SGEMM throughput measured in the same run (the driver's peak file has
+             HBM and bf16 only).
 `cpu_baseline` the reference's own per-ray routine (src/cuda/rtKernels.cu) compiled
-             for the host (oracle/_ref), OpenMP over all host cores, timed on a
-             bounded sample of the same sweep.
+             for the host (oracle/_ref), OpenMP over all host cores, timed on a bounded
+             random sample of (angle, frequency) samples of the same sweep.
 Under torchrun (N > 1) every rank sweeps its own angle set (phi offset by
 rank * 0.1 deg): weak scaling, no collective on the data path; the time is the
 max over ranks.
@@ -45,16 +54,34 @@ FLOP_PER_BOX = 27
 FLOP_PER_TRI = 57
 
 
-def workload(rank: int = 0):
+def workload(name: str, rank: int = 0):
+    """Mesh, angles, frequencies and ray grids of a benchmark workload."""
     from sagittasbr_b200 import meshes as M
-    v, t = M.trihedral(1.0, 100)
+    if name == "trihedral":
+        v, t = M.trihedral(1.0, 100)
+        th, ph = np.meshgrid(np.arange(0.0, 91.0), np.arange(0.0, 91.0), indexing="ij")
+        th, ph = th.ravel(), ph.ravel()
+        freqs, mb = [1e10], 3
+    elif name == "sphere":
+        v, t = M.icosphere(5, 1.0)
+        ph = np.arange(0.0, 360.0)
+        th = np.full(ph.size, 90.0)
+        freqs, mb = [1e9], 3
+    elif name in ("aircraft", "aircraft-dev"):
+        v, t = M.aircraft(seed=1)
+        nf, step = (64, 0.5) if name == "aircraft" else (8, 5.0)
+        ph = np.arange(0.0, 360.0 + 1e-9, step)
+        th = np.full(ph.size, 90.0)
+        freqs, mb = list(np.geomspace(1e9, 18e9, nf)), 5
+    else:
+        raise ValueError(name)
+    ph = ph + 0.1 * rank
     G = 2.0 * M.bounding_radius(v)
-    n = M.rays_for(1e10, G)
-    th, ph = np.meshgrid(np.arange(0.0, 91.0), np.arange(0.0, 91.0), indexing="ij")
-    th = th.ravel()
-    ph = ph.ravel() + 0.1 * rank
-    return dict(verts=v, tris=t, theta=th, phi=ph, freqs=[1e10], nx=n, ny=n, G=G, max_bounces=3, R=1.0,
-                name=f"trihedral_60k_10GHz_{n}x{n}_3b_{th.size}ang")
+    grid = {f: M.rays_for(f, G) for f in freqs}
+    n = grid[max(freqs)]
+    label = f"{name}_{t.shape[0]}tri_{len(freqs)}f_{min(freqs)/1e9:g}-{max(freqs)/1e9:g}GHz_{n}x{n}_{mb}b_{th.size}ang"
+    return dict(verts=v, tris=t, theta=th, phi=ph, freqs=freqs, grid=grid, nx=n, ny=n, G=G, max_bounces=mb,
+                R=1.0, name=label, workload=name)
 
 
 def dist_env():
@@ -127,32 +154,39 @@ def fp32_peak_tflops(torch) -> float:
 
 
 def cpu_reference(w, budget_s: float, threads: int = 0, want_counts: bool = True):
-    """The reference's own per-ray code (oracle/_ref) on a bounded sample of the
-    sweep; returns (samples/s, bounces/s, sample description, V_box, V_tri)."""
+    """The reference's own per-ray code (oracle/_ref) on a bounded random sample of
+    (angle, frequency) samples, each on its own grid as the reference runs them;
+    returns (samples/s, bounces/s, sample description, V_box, V_tri, kind)."""
     from oracle import oracle as O
     kind = "32fast" if O.ref_available("32fast") else None
-    idx = np.random.default_rng(7).permutation(w["theta"].size)
+    rng = np.random.default_rng(7)
+    na, nf = w["theta"].size, len(w["freqs"])
+    order = rng.permutation(na * nf)
     done, bounces, t_used = 0, 0, 0.0
-    while t_used < budget_s and done < idx.size:
-        sel = idx[done:done + 4]
+    while t_used < budget_s and done < order.size:
+        s = int(order[done])
+        a, f = divmod(s, nf)
+        fr = w["freqs"][f]
+        n = w["grid"][fr]
         t0 = time.perf_counter()
         if kind:
-            out = O.ref_sweep(w["verts"], w["tris"], w["theta"][sel], w["phi"][sel], w["freqs"], w["nx"], w["ny"],
-                              w["G"], w["max_bounces"], w["R"], kind=kind, threads=threads)
+            out = O.ref_sweep(w["verts"], w["tris"], w["theta"][a:a + 1], w["phi"][a:a + 1], [fr], n, n, w["G"],
+                              w["max_bounces"], w["R"], kind=kind, threads=threads)
         else:
-            out = O.sweep(w["verts"], w["tris"], w["theta"][sel], w["phi"][sel], w["freqs"], w["nx"], w["ny"],
-                          w["G"], w["max_bounces"], w["R"], precision=32, threads=threads)
+            out = O.sweep(w["verts"], w["tris"], w["theta"][a:a + 1], w["phi"][a:a + 1], [fr], n, n, w["G"],
+                          w["max_bounces"], w["R"], precision=32, threads=threads)
         t_used += time.perf_counter() - t0
         bounces += int(out.counts["bounces"].sum())
-        done += sel.size
+        done += 1
     vbox = vtri = None
     if want_counts:
-        sel = idx[:2]
-        o = O.sweep(w["verts"], w["tris"], w["theta"][sel], w["phi"][sel], w["freqs"], w["nx"], w["ny"], w["G"],
+        sel = rng.permutation(na)[:2]
+        fr = w["freqs"][0]
+        o = O.sweep(w["verts"], w["tris"], w["theta"][sel], w["phi"][sel], [fr], w["grid"][fr], w["grid"][fr], w["G"],
                     w["max_bounces"], w["R"], precision=64, accel="tree", threads=threads)
         q = o.counts["queries"].sum()
         vbox, vtri = float(o.counts["box_tests"].sum() / q), float(o.counts["tri_tests"].sum() / q)
-    sample = (f"{done} of {w['theta'].size} angles (random, seed 7) at full {w['nx']}x{w['ny']} rays, "
+    sample = (f"{done} random (angle, frequency) samples of {na * nf}, each on its own n_f x n_f grid, "
               f"{'reference rtKernels.cu host build (oracle/_ref, FP32, -O3)' if kind else 'FP32 oracle port'}")
     return done / t_used, bounces / t_used, sample, vbox, vtri, ("reference" if kind else "port")
 
@@ -175,14 +209,10 @@ def run_reference_arm(args):
     ws, rank, _ = dist_env()
     if rank != 0:
         return 0
-    w = workload(0)
+    w = workload(args.workload, 0)
     threads = os.cpu_count() or 1
-    for _ in range(args.warmup):
-        pass
-    per_step = []
-    bps = []
-    sample = ""
-    kind = "port"
+    per_step, bps = [], []
+    sample, kind = "", "port"
     budget = max(2.0, 60.0 / max(1, args.steps + args.warmup))
     for s in range(args.warmup + args.steps):
         sps, bounces, sample, _, _, kind = cpu_reference(w, budget, threads, want_counts=False)
@@ -193,9 +223,9 @@ def run_reference_arm(args):
     line = {
         "impl": "reference", "metric": "angle-freq samples/s", "value": v, "unit": "samples/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * w["theta"].size / v, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded trihedral mesh)",
-        "config": {"workload": w["name"], "angles": int(w["theta"].size), "rays_per_angle": w["nx"] * w["ny"],
+        "ms_per_step": 1e3 * w["theta"].size * len(w["freqs"]) / v, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": f"synthetic (seeded {args.workload} mesh)",
+        "config": {"workload": w["name"], "angles": int(w["theta"].size), "freqs": len(w["freqs"]),
                    "max_bounces": w["max_bounces"], "sampled": True},
         "mray_bounces_per_s": float(np.mean(bps)) / 1e6,
         "cpu_baseline": {"value": v, "unit": "samples/s", "cores": threads, "kind": kind, "sample": sample},
@@ -211,12 +241,15 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="trihedral", choices=["trihedral", "sphere", "aircraft", "aircraft-dev"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--angles", type=int, default=0,
                     help="profile case: trace only this many angles, evenly spread over the sweep")
     ap.add_argument("--no-per-angle", action="store_true", help="skip the per-angle mode measurement")
     ap.add_argument("--per-angle-stride", type=int, default=8,
                     help="per-angle mode is timed on every n-th angle of the sweep")
+    ap.add_argument("--fp64-check", type=int, default=0,
+                    help="compare with a full-FP64 run of the batched job on this many angles")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -232,7 +265,7 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
-    w = workload(rank)
+    w = workload(args.workload, rank)
     if args.angles > 0:
         pick = np.linspace(0, w["theta"].size - 1, args.angles).round().astype(int)
         w["theta"], w["phi"] = w["theta"][pick], w["phi"][pick]
@@ -242,7 +275,9 @@ def main():
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     sp = stream.cuda_stream
+    t_scene = time.perf_counter()
     scene = sbr.Scene(w["verts"], w["tris"], device=local)
+    scene_s = time.perf_counter() - t_scene
     job = sbr.JobSpec(w["theta"], w["phi"], w["freqs"], w["nx"], w["ny"], w["G"], w["max_bounces"], w["R"])
     plan = sbr.Plan(scene, [job], mode=sbr.MODE_BATCHED, precision=sbr.PREC_MIXED, stream=sp)
     info = plan.info
@@ -285,6 +320,7 @@ def main():
 
     # end to end through sbr_run (host arrays in, host arrays out)
     e2e_ms = []
+    r2 = None
     for s in range(1 + min(args.steps, 3)):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -297,14 +333,13 @@ def main():
     e2e_value = samples * ws / (float(e2e_t[0]) * 1e-3)
     assert np.array_equal(r2.field, res.field), "sbr_run and plan results differ"
 
-    # per-angle mode (the reference's loop structure) on a subset of the same sweep
+    # per-angle mode: the reference's loop structure, each frequency on its own grid
     per_angle = None
     if not args.no_per_angle:
         sub = slice(0, None, args.per_angle_stride)
-        pjob = sbr.JobSpec(w["theta"][sub], w["phi"][sub], w["freqs"], w["nx"], w["ny"], w["G"], w["max_bounces"],
-                           w["R"])
-        pplan = sbr.Plan(scene, [pjob], mode=sbr.MODE_PER_ANGLE, precision=sbr.PREC_FP32, stream=sp)
-        pplan.execute()
+        pjobs = [sbr.JobSpec(w["theta"][sub], w["phi"][sub], [f], w["grid"][f], w["grid"][f], w["G"],
+                             w["max_bounces"], w["R"]) for f in w["freqs"]]
+        pplan = sbr.Plan(scene, pjobs, mode=sbr.MODE_PER_ANGLE, precision=sbr.PREC_FP32, stream=sp)
         torch.cuda.synchronize()
         pa0, pa1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         pa0.record(stream)
@@ -314,14 +349,39 @@ def main():
         pa_ms = pa0.elapsed_time(pa1)
         per_angle_value = pplan.info["n_samples"] / (pa_ms * 1e-3)
         pres = pplan.results()
-        bplan = sbr.Plan(scene, [pjob], mode=sbr.MODE_BATCHED, precision=sbr.PREC_MIXED, stream=sp)
-        bplan.execute()
-        bres = bplan.results()
-        field_rel = float(np.abs(pres.field - bres.field).max() / np.abs(bres.field).max())
+        # the same angles through the batched engine, for the field comparison
+        bjob = sbr.JobSpec(w["theta"][sub], w["phi"][sub], w["freqs"], w["nx"], w["ny"], w["G"], w["max_bounces"],
+                           w["R"])
+        bres = sbr.run(scene, bjob, mode=sbr.MODE_BATCHED, precision=sbr.PREC_MIXED)
+        nsub, nf = len(w["theta"][sub]), len(w["freqs"])
+        pf = pres.field.reshape(nf, nsub).T  # per-angle plan is frequency-major (one job per frequency)
+        bf = bres.field.reshape(nsub, nf)
+        same_grid = all(w["grid"][f] == w["nx"] for f in w["freqs"])
         per_angle = {"value": per_angle_value, "unit": "samples/s", "precision": "fp32 (reference arithmetic)",
-                     "angles": pplan.info["n_samples"], "ms": pa_ms, "launches": pplan.info["launches_per_execute"],
-                     "max_field_err_vs_batched_rel_to_max": field_rel,
-                     "batched_speedup": value / ws / per_angle_value}
+                     "samples": pplan.info["n_samples"], "angles": nsub, "ms": pa_ms,
+                     "launches": pplan.info["launches_per_execute"],
+                     "rays_launched": pplan.info["n_rays_clipped"],
+                     "batched_speedup": value / ws / per_angle_value,
+                     "grids": "same as batched" if same_grid else "own grid per frequency (batched: finest grid)",
+                     "max_field_diff_vs_batched_rel_to_max": float(np.abs(pf - bf).max() / np.abs(bf).max())}
+        pplan.close()
+
+    # batched mixed precision against a full-FP64 run of the same batched job
+    fp64 = None
+    if args.fp64_check > 0:
+        pick = np.linspace(0, w["theta"].size - 1, args.fp64_check).round().astype(int)
+        cjob = sbr.JobSpec(w["theta"][pick], w["phi"][pick], w["freqs"], w["nx"], w["ny"], w["G"], w["max_bounces"],
+                           w["R"])
+        a = sbr.run(scene, cjob, mode=sbr.MODE_BATCHED, precision=sbr.PREC_MIXED)
+        b = sbr.run(scene, cjob, mode=sbr.MODE_BATCHED, precision=sbr.PREC_FP64)
+        ddb = np.abs(a.rcs_dbsm - b.rcs_dbsm)
+        peak = b.rcs_dbsm.reshape(len(pick), -1).max(axis=0)[None, :]
+        lit = (b.rcs_dbsm.reshape(len(pick), -1) > peak - 30.0).ravel()
+        fp64 = {"samples": int(ddb.size), "max_abs_ddb": float(ddb.max()), "p99_abs_ddb": float(np.percentile(ddb, 99)),
+                "frac_within_0.1dB": float((ddb <= 0.1).mean()),
+                "max_abs_ddb_within_30dB_of_peak": float(ddb[lit].max()),
+                "max_field_diff_rel_to_max": float(np.abs(a.field - b.field).max() / np.abs(b.field).max()),
+                "fp64_ms": b.device_ms, "mixed_ms": a.device_ms}
 
     if dist is not None:
         dist.barrier()
@@ -336,14 +396,14 @@ def main():
     cpu = None
     vbox = vtri = None
     if not args.no_cpu and ws == 1:
-        sps, bps, sample, vbox, vtri, kind = cpu_reference(w, 15.0)
+        sps, bps, sample, vbox, vtri, kind = cpu_reference(w, 15.0, want_counts=args.workload != "aircraft")
         cpu = {"value": sps, "unit": "samples/s", "cores": os.cpu_count(), "kind": kind, "sample": sample,
                "mray_bounces_per_s": bps / 1e6}
     roof = None
     if vbox is not None:
         flop_q = FLOP_PER_BOX * vbox + FLOP_PER_TRI * vtri
         achieved = queries_step * flop_q / (kern_ms * 1e-3) / 1e12
-        traffic = read_traffic()
+        traffic = read_traffic() if args.workload == "trihedral" else None
         roof = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                 "traffic": traffic, "kernel": "k_trace (persistent) + k_finalize",
                 "flop_per_query": flop_q, "v_box": vbox, "v_tri": vtri, "queries_per_launch": queries_step,
@@ -355,16 +415,18 @@ def main():
         "metric": "angle-freq samples/s", "value": value, "unit": "samples/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32 traversal + fp64 phase/sums",
-        "data": "synthetic (seeded trihedral mesh)",
+        "data": f"synthetic (seeded {args.workload} mesh)",
         "config": {"workload": w["name"], "angles": int(w["theta"].size), "freqs": len(w["freqs"]),
-                   "rays_per_angle": w["nx"] * w["ny"], "rays_launched_per_step": info["n_rays_clipped"],
-                   "max_bounces": w["max_bounces"], "mode": "batched persistent", "precision": "mixed",
+                   "triangles": int(w["tris"].shape[0]), "rays_per_angle": w["nx"] * w["ny"],
+                   "rays_launched_per_step": info["n_rays_clipped"], "max_bounces": w["max_bounces"],
+                   "mode": "batched persistent", "precision": "mixed",
                    "l2": "flushed before every step (256 MiB write inside the timed region)",
-                   "parallelism": f"{ws} GPU(s), independent sweeps"},
+                   "parallelism": f"{ws} GPU(s), independent sweeps", "scene_build_s": scene_s},
         "mray_bounces_per_s": bounces_step * ws / (step_ms * 1e-3) / 1e6,
         "closest_hit_queries_per_s": queries_step * ws / (step_ms * 1e-3),
         "kernel_ms": kern_ms,
         "per_angle": per_angle,
+        "fp64_check": fp64,
         "e2e": {"value": e2e_value, "unit": "samples/s", "h2d_bytes_per_step": info["h2d_bytes"],
                 "d2h_bytes_per_step": info["d2h_bytes"], "ms_per_step": float(e2e_t[0])},
         "gpu_launches": int(info["launches_per_execute"]) * args.steps,

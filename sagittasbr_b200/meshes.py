@@ -150,6 +150,123 @@ def box(size: float = 1.0):
     return V.astype(np.float32), T.astype(np.uint32)
 
 
+def _grid_tris(nu: int, nv: int, offset: int = 0, wrap_v: bool = False, flip: bool = False):
+    """Two triangles per cell of an (nu+1) x (nv+1) vertex grid (row-major, u slow).
+    With wrap_v the last column connects back to the first (nv columns of vertices)."""
+    cols = nv if wrap_v else nv + 1
+    u = np.arange(nu)[:, None]
+    v = np.arange(nv)[None, :]
+    a = offset + u * cols + v
+    b = offset + (u + 1) * cols + v
+    vn = (v + 1) % cols if wrap_v else v + 1
+    c = offset + (u + 1) * cols + vn
+    d = offset + u * cols + vn
+    t1 = np.stack([a, b, c], axis=-1).reshape(-1, 3)
+    t2 = np.stack([a, c, d], axis=-1).reshape(-1, 3)
+    T = np.empty((t1.shape[0] * 2, 3), dtype=np.int64)
+    T[0::2], T[1::2] = t1, t2
+    if flip:
+        T[:, [1, 2]] = T[:, [2, 1]]
+    return T
+
+
+def _orient_by_normal(V, T, want):
+    """Flip the whole component if its mean normal disagrees with `want` (a vector
+    field evaluated at the triangle centroids, pointing to the outside)."""
+    a, b, c = V[T[:, 0]], V[T[:, 1]], V[T[:, 2]]
+    n = np.cross(b - a, c - a)
+    w = want((a + b + c) / 3.0)
+    if np.einsum("ij,ij->", n, w) < 0:
+        T = T[:, [0, 2, 1]]
+    return T
+
+
+def superellipsoid_fuselage(length: float = 20.0, radius: float = 1.5, n_eta: int = 1000, n_omega: int = 600,
+                            e1: float = 0.3):
+    """Closed body of revolution along x: x = L/2 s(eta)^e1, r = R c(eta)^e1 with
+    s/c the signed powers of sin/cos (a superellipsoid blunted by e1 < 1); circular
+    cross-section.  Poles are closed with triangle fans."""
+    def spow(x, e):
+        return np.sign(x) * np.abs(x) ** e
+    eta = np.linspace(-np.pi / 2, np.pi / 2, n_eta + 1)[1:-1]   # interior rings
+    om = np.linspace(0.0, 2 * np.pi, n_omega, endpoint=False)
+    E, O = np.meshgrid(eta, om, indexing="ij")
+    x = 0.5 * length * spow(np.sin(E), e1)
+    r = radius * spow(np.cos(E), e1)
+    V = np.stack([x, r * np.cos(O), r * np.sin(O)], axis=-1).reshape(-1, 3)
+    nr = eta.size
+    T = [_grid_tris(nr - 1, n_omega, 0, wrap_v=True)]
+    tail = V.shape[0]
+    nose = tail + 1
+    V = np.concatenate([V, [[-0.5 * length, 0, 0], [0.5 * length, 0, 0]]])
+    j = np.arange(n_omega)
+    jn = (j + 1) % n_omega
+    T.append(np.stack([np.full(n_omega, tail), jn, j], axis=1))
+    last = (nr - 1) * n_omega
+    T.append(np.stack([np.full(n_omega, nose), last + j, last + jn], axis=1))
+    T = np.concatenate(T)
+    T = _orient_by_normal(V, T, lambda p: p * np.array([0.0, 1.0, 1.0]))
+    return V, T
+
+
+def _naca_half_thickness(xi, t):
+    """Half thickness of a symmetric 4-digit NACA section (closed trailing edge)."""
+    return 5.0 * t * (0.2969 * np.sqrt(xi) - 0.1260 * xi - 0.3516 * xi ** 2 + 0.2843 * xi ** 3 - 0.1036 * xi ** 4)
+
+
+def trapezoid_surface(span: float, root_chord: float, tip_chord: float, sweep_deg: float, thickness: float,
+                      n_chord: int, n_span: int, origin, span_axis, thick_axis):
+    """Closed swept trapezoidal lifting surface (upper + lower skins meeting at the
+    leading and trailing edges, tip closed).  Chord along +x from the leading edge at
+    `origin`; span along `span_axis` (unit vector); thickness along `thick_axis`."""
+    xi = 0.5 * (1.0 - np.cos(np.linspace(0.0, np.pi, n_chord + 1)))    # cosine spacing
+    eta = np.linspace(0.0, 1.0, n_span + 1)
+    XI, ET = np.meshgrid(xi, eta, indexing="ij")
+    chord = root_chord + (tip_chord - root_chord) * ET
+    # the tip station is pinched to zero thickness so the two skins close there
+    h = _naca_half_thickness(XI, thickness) * chord * np.minimum(1.0, (1.0 - ET) * n_span)
+    xle = ET * span * np.tan(np.radians(sweep_deg))
+    o = np.asarray(origin, dtype=np.float64)
+    sa, ta = np.asarray(span_axis, float), np.asarray(thick_axis, float)
+    base = o + (xle + XI * chord)[..., None] * np.array([1.0, 0, 0]) + (ET * span)[..., None] * sa
+    up = (base + h[..., None] * ta).reshape(-1, 3)
+    lo = (base - h[..., None] * ta).reshape(-1, 3)
+    V = np.concatenate([up, lo])
+    nv = up.shape[0]
+    Tu = _grid_tris(n_chord, n_span, 0)
+    Tl = _grid_tris(n_chord, n_span, nv, flip=True)
+    # orient each skin so its normals point away from the chord plane
+    Tu = _orient_by_normal(V, Tu, lambda p: np.broadcast_to(ta, p.shape))
+    Tl = _orient_by_normal(V, Tl, lambda p: np.broadcast_to(-ta, p.shape))
+    return V, np.concatenate([Tu, Tl])
+
+
+def aircraft(seed: int = 1, jitter: float = 1e-3, fuselage=(1000, 600), wing=(100, 1000), tail=(50, 250)):
+    """Seeded aircraft-like mesh (about 2.15 M triangles at the default resolution):
+    superellipsoid fuselage 20 m long with 1.5 m semi-axes, swept trapezoidal wings
+    (18 m span, chord 3 m -> 1 m, 25 deg sweep, 12 % thick), horizontal tail
+    (6.4 m span) and a vertical fin, Gaussian vertex jitter (sigma = `jitter`),
+    outward winding, centred on its bounding box."""
+    parts = [superellipsoid_fuselage(20.0, 1.5, *fuselage)]
+    nc, ns = wing
+    for side in (1.0, -1.0):
+        parts.append(trapezoid_surface(9.0, 3.0, 1.0, 25.0, 0.12, nc, ns, (-2.0, 0.0, -0.5), (0, side, 0), (0, 0, 1)))
+    tc, ts = tail
+    for side in (1.0, -1.0):
+        parts.append(trapezoid_surface(3.2, 2.0, 0.8, 30.0, 0.10, tc, ts, (6.8, 0.0, 0.3), (0, side, 0), (0, 0, 1)))
+    parts.append(trapezoid_surface(3.0, 2.5, 1.0, 35.0, 0.10, tc, ts, (6.5, 0.0, 0.9), (0, 0, 1), (0, 1, 0)))
+    Vs, Ts, off = [], [], 0
+    for V, T in parts:
+        Vs.append(V)
+        Ts.append(T + off)
+        off += V.shape[0]
+    V = np.concatenate(Vs)
+    T = np.concatenate(Ts)
+    if jitter > 0:
+        V = V + np.random.default_rng(seed).normal(0.0, jitter, V.shape)
+    return centre_on_aabb(V), T.astype(np.uint32)
+
+
 def bounding_radius(verts) -> float:
     """Radius of the bounding sphere about the AABB centre."""
     v = np.asarray(verts, dtype=np.float64)
