@@ -248,6 +248,8 @@ def main():
     ap.add_argument("--no-per-angle", action="store_true", help="skip the per-angle mode measurement")
     ap.add_argument("--per-angle-stride", type=int, default=8,
                     help="per-angle mode is timed on every n-th angle of the sweep")
+    ap.add_argument("--first-hit", default="traverse", choices=["traverse", "raster"],
+                    help="first closest hit by BVH walk (default) or by the first-hit raster")
     ap.add_argument("--fp64-check", type=int, default=0,
                     help="compare with a full-FP64 run of the batched job on this many angles")
     args = ap.parse_args()
@@ -279,7 +281,8 @@ def main():
     scene = sbr.Scene(w["verts"], w["tris"], device=local)
     scene_s = time.perf_counter() - t_scene
     job = sbr.JobSpec(w["theta"], w["phi"], w["freqs"], w["nx"], w["ny"], w["G"], w["max_bounces"], w["R"])
-    plan = sbr.Plan(scene, [job], mode=sbr.MODE_BATCHED, precision=sbr.PREC_MIXED, stream=sp)
+    first_hit = sbr.FIRST_HIT_RASTER if args.first_hit == "raster" else sbr.FIRST_HIT_TRAVERSE
+    plan = sbr.Plan(scene, [job], mode=sbr.MODE_BATCHED, precision=sbr.PREC_MIXED, stream=sp, first_hit=first_hit)
     info = plan.info
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
@@ -324,7 +327,7 @@ def main():
     for s in range(1 + min(args.steps, 3)):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        r2 = sbr.run(scene, job, mode=sbr.MODE_BATCHED, precision=sbr.PREC_MIXED)
+        r2 = sbr.run(scene, job, mode=sbr.MODE_BATCHED, precision=sbr.PREC_MIXED, first_hit=first_hit)
         if s:
             e2e_ms.append((time.perf_counter() - t0) * 1e3)
     e2e_t = torch.tensor([float(np.mean(e2e_ms))], device="cuda", dtype=torch.float64)

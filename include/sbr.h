@@ -113,6 +113,17 @@ typedef struct sbr_job {
 #define SBR_PREC_FP32 1       /* the reference FP32 build's arithmetic (launch plane at 10 G, FP32 phase) */
 #define SBR_PREC_FP64 2       /* everything in FP64 (the reference USE_DOUBLE build's arithmetic) */
 
+/* How the first closest hit of each ray is found.  Primary rays of one angle are
+ * parallel and start on the launcher grid, so their first hits form an
+ * orthographic z-buffer: RASTER tests every triangle against the pixels its
+ * projection covers (same Moller-Trumbore arithmetic) and keeps the nearest per
+ * pixel; later bounces always walk the BVH.  RASTER applies to batched FP32 /
+ * mixed runs (per-angle and FP64 runs always walk).  Measured on B200 it costs
+ * about as much as the walk it replaces for coherent ray tubes, so the default
+ * walks. */
+#define SBR_FIRST_HIT_TRAVERSE 0  /* walk the BVH for every query (default) */
+#define SBR_FIRST_HIT_RASTER 1    /* first hits from the orthographic first-hit raster */
+
 #define SBR_POL_SCALAR 0      /* the reference's scalar PO term (HH == VV) */
 #define SBR_POL_HHVV 1        /* PEC E-vector tracking; fields for HH and VV */
 
@@ -123,7 +134,8 @@ typedef struct sbr_run_opts {
     int32_t use_graph;        /* capture plan execution in a CUDA graph (batched mode) */
     void* stream;             /* cudaStream_t to launch on; NULL -> the scene's own stream */
     int32_t ctas_per_sm;      /* persistent grid size per SM; 0 -> occupancy-derived */
-    int32_t reserved[7];
+    int32_t first_hit;        /* SBR_FIRST_HIT_* */
+    int32_t reserved[6];
 } sbr_run_opts;
 
 /* Results for every (job, angle, frequency[, polarization]) in job order, then

@@ -23,12 +23,13 @@ from typing import Sequence
 import numpy as np
 
 from . import _lib
-from ._lib import (MODE_BATCHED, MODE_PER_ANGLE, POL_HHVV, POL_SCALAR, PREC_FP32, PREC_FP64, PREC_MIXED,
-                   SbrError, check, lib)
+from ._lib import (FIRST_HIT_RASTER, FIRST_HIT_TRAVERSE, MODE_BATCHED, MODE_PER_ANGLE, POL_HHVV, POL_SCALAR,
+                   PREC_FP32, PREC_FP64, PREC_MIXED, SbrError, check, lib)
 
 __all__ = [
     "Scene", "JobSpec", "SweepResult", "Plan", "run", "trace_records", "load_config", "config_angles",
     "load_obj", "write_csv", "run_sweep", "SbrError", "MODE_BATCHED", "MODE_PER_ANGLE", "PREC_MIXED",
+    "FIRST_HIT_RASTER", "FIRST_HIT_TRAVERSE",
     "PREC_FP32", "PREC_FP64", "POL_SCALAR", "POL_HHVV", "RAY_RECORD",
 ]
 
@@ -151,12 +152,14 @@ class SweepResult:
         return int(self.stats[:, 3].sum())
 
 
-def _opts(mode, precision, polarization=POL_SCALAR, stream=None, use_graph=False, ctas_per_sm=0):
+def _opts(mode, precision, polarization=POL_SCALAR, stream=None, use_graph=False, ctas_per_sm=0,
+          first_hit=FIRST_HIT_TRAVERSE):
     o = _lib.RunOpts()
     o.mode, o.precision, o.polarization = int(mode), int(precision), int(polarization)
     o.use_graph = 1 if use_graph else 0
     o.stream = stream
     o.ctas_per_sm = int(ctas_per_sm)
+    o.first_hit = int(first_hit)
     return o
 
 
@@ -171,11 +174,12 @@ class Plan:
     """Prepared sweep (sbr_plan): frames, work items and result buffers on the GPU."""
 
     def __init__(self, scene: Scene, jobs: Sequence[JobSpec], mode=MODE_BATCHED, precision=PREC_MIXED,
-                 stream=None, use_graph=False, ctas_per_sm=0):
+                 stream=None, use_graph=False, ctas_per_sm=0, first_hit=None):
         self.scene = scene
         self.jobs = list(jobs)
         self._jc = _jobs_c(self.jobs)
-        o = _opts(mode, precision, stream=stream, use_graph=use_graph, ctas_per_sm=ctas_per_sm)
+        o = _opts(mode, precision, stream=stream, use_graph=use_graph, ctas_per_sm=ctas_per_sm,
+                  first_hit=FIRST_HIT_TRAVERSE if first_hit is None else first_hit)
         h = C.c_void_p()
         check(lib().sbr_plan_create(scene.handle, self._jc, len(self.jobs), C.byref(o), C.byref(h)),
               "sbr_plan_create")
@@ -217,7 +221,7 @@ class Plan:
 
 
 def run(scene: Scene, jobs: Sequence[JobSpec] | JobSpec, mode=MODE_BATCHED, precision=PREC_MIXED,
-        stream=None) -> SweepResult:
+        stream=None, first_hit=None) -> SweepResult:
     """One call through sbr_run: host arrays in, host arrays out."""
     if isinstance(jobs, JobSpec):
         jobs = [jobs]
@@ -230,16 +234,16 @@ def run(scene: Scene, jobs: Sequence[JobSpec] | JobSpec, mode=MODE_BATCHED, prec
     st = np.zeros(4 * na, dtype=np.uint64)
     r = _lib.Result()
     r.field, r.sigma_m2, r.rcs_dbsm, r.stats = f.ctypes.data, s.ctypes.data, d.ctypes.data, st.ctypes.data
-    o = _opts(mode, precision, stream=stream)
+    o = _opts(mode, precision, stream=stream, first_hit=FIRST_HIT_TRAVERSE if first_hit is None else first_hit)
     check(lib().sbr_run(scene.handle, jc, len(jobs), C.byref(r), C.byref(o)), "sbr_run")
     return SweepResult(f[0::2] + 1j * f[1::2], s, d, st.reshape(na, 4), r.device_ms)
 
 
-def trace_records(scene: Scene, job: JobSpec, precision=PREC_MIXED) -> np.ndarray:
+def trace_records(scene: Scene, job: JobSpec, precision=PREC_MIXED, first_hit=None) -> np.ndarray:
     """Per-ray hit records [n_angles, ny, nx] (sbr_trace_records)."""
     jc = job.to_c()
     out = np.zeros((job.n_angles, job.ny, job.nx), dtype=RAY_RECORD)
-    o = _opts(MODE_BATCHED, precision)
+    o = _opts(MODE_BATCHED, precision, first_hit=FIRST_HIT_TRAVERSE if first_hit is None else first_hit)
     check(lib().sbr_trace_records(scene.handle, C.byref(jc), C.byref(o), _p(out)), "sbr_trace_records")
     return out
 

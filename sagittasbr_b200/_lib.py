@@ -15,6 +15,7 @@ STATUS_NAMES = {
     12: "SBR_ERR_IO", 13: "SBR_ERR_PARSE", 14: "SBR_ERR_UNSUPPORTED",
 }
 MODE_BATCHED, MODE_PER_ANGLE = 0, 1
+FIRST_HIT_TRAVERSE, FIRST_HIT_RASTER = 0, 1
 PREC_MIXED, PREC_FP32, PREC_FP64 = 0, 1, 2
 POL_SCALAR, POL_HHVV = 0, 1
 MAX_REC = 16
@@ -69,7 +70,8 @@ class RunOpts(C.Structure):
         ("use_graph", C.c_int32),
         ("stream", C.c_void_p),
         ("ctas_per_sm", C.c_int32),
-        ("reserved", C.c_int32 * 7),
+        ("first_hit", C.c_int32),
+        ("reserved", C.c_int32 * 6),
     ]
 
 

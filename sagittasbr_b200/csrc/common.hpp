@@ -30,16 +30,16 @@ enum : uint32_t {
 };
 
 // ------------------------------------------------------------- GPU layout
-// Binary BVH with both child boxes stored in the parent (one 64 B node = four
-// 16 B loads).  Child reference: >= 0 inner node index; < 0 leaf, where
-// ~ref = first_triangle * 16 + count (count 1..15).
-struct __align__(16) GNode {
-    float4 a;     // child 0: lo.x hi.x lo.y hi.y
-    float4 b;     // child 1: lo.x hi.x lo.y hi.y
-    float4 c;     // child 0 lo.z hi.z, child 1 lo.z hi.z
-    int4 link;    // ref0, ref1, unused, unused
+// 4-wide BVH node: the boxes of up to four children in structure-of-arrays form
+// (each float4 holds one plane of all four children) and their references, seven
+// 16 B loads.  Child reference: >= 0 inner node index; < 0 leaf, where
+// ~ref = first_triangle * 16 + count (count 1..15).  Empty slots hold a point box
+// far outside any ray's reach (it never passes the slab test) and reference ~0.
+struct __align__(16) GNode4 {
+    float4 lox, hix, loy, hiy, loz, hiz;
+    int4 child;
 };
-static_assert(sizeof(GNode) == 64, "GNode must be 64 bytes");
+static_assert(sizeof(GNode4) == 112, "GNode4 must be 112 bytes");
 
 constexpr int kLeafMax = 15;
 constexpr int kStackDepth = 64;     // reference uses 64 (src/cuda/rtKernels.cu:65)
@@ -58,7 +58,7 @@ struct GTri64 {
 };
 
 struct SceneView {
-    const GNode* __restrict__ nodes;
+    const GNode4* __restrict__ nodes;
     const GTri* __restrict__ tris;
     const GTri64* __restrict__ tris64;
     const int32_t* __restrict__ tri_id;
@@ -84,6 +84,10 @@ struct __align__(16) Segment {
     int32_t pad;
     int64_t item_base;    // first work item of this segment
     int64_t sample_base;  // first output sample (angle, freq) index
+    // pixel coordinates of a point P on the launcher grid: s = ps[0..2].P + ps[3],
+    // t = pt[0..2].P + pt[3] (pixel (i, j) is centred at s = i, t = j)
+    double ps[4], pt[4];
+    int64_t zbase;        // first first-hit buffer entry of this segment within its chunk
 };
 struct JobConst {
     int32_t nx, ny;

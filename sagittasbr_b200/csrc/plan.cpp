@@ -92,6 +92,7 @@ void release(sbr_plan* p) {
     cudaFree(p->d_field);
     cudaFree(p->d_stats);
     cudaFree(p->d_queue);
+    cudaFree(p->d_zbuf);
     if (p->ev0) cudaEventDestroy(p->ev0);
     if (p->ev1) cudaEventDestroy(p->ev1);
     delete p;
@@ -237,6 +238,14 @@ sbr_status build_tables(const sbr_scene* s, const sbr_job* jobs, size_t n_jobs, 
                 }
             }
             g.shift = shift;
+            // pixel coordinates on the launcher: s(P) = (P - llc).U / |U|^2 * nx - 1/2
+            for (int k = 0; k < 3; ++k) {
+                g.ps[k] = fd.u[k] / uu * J.nx;
+                g.pt[k] = fd.v[k] / vv * J.ny;
+            }
+            g.ps[3] = -(fd.llc[0] * g.ps[0] + fd.llc[1] * g.ps[1] + fd.llc[2] * g.ps[2]) - 0.5;
+            g.pt[3] = -(fd.llc[0] * g.pt[0] + fd.llc[1] * g.pt[1] + fd.llc[2] * g.pt[2]) - 0.5;
+            g.zbase = 0;
             g.job = (int32_t)j;
             g.angle = (int32_t)a;
             int bx = (g.ni + kBlockW - 1) / kBlockW, by = (g.nj + kBlockH - 1) / kBlockH;
@@ -327,8 +336,44 @@ sbr_status sbr_plan_create(sbr_scene* s, const sbr_job* jobs, size_t n_jobs, con
     p->n_rays_clipped = tot.n_rays_clipped;
     p->n_rays_grid = tot.n_rays_grid;
 
+    // first-hit rasterisation (batched FP32 / mixed): chunks of consecutive
+    // segments whose per-pixel first-hit buffers fit a fixed budget
+    p->raster = o.mode == SBR_MODE_BATCHED && o.precision != SBR_PREC_FP64 && o.first_hit == SBR_FIRST_HIT_RASTER &&
+                p->n_items > 0;
+    if (p->raster) {
+        const int64_t budget = int64_t(256) << 20;  // entries (8 B each): 2 GiB
+        sbr_plan::Chunk c{0, 0, 0, 0, 0};
+        for (size_t g = 0; g < p->segs.size(); ++g) {
+            const int64_t px = (int64_t)p->segs[g].ni * p->segs[g].nj;
+            // (the raster launch's grid.y is the chunk's segment count: at most 65535)
+            if (c.seg_end > c.seg_begin && (c.zcount + px > budget || c.seg_end - c.seg_begin >= 65535)) {
+                c.item_end = p->seg_base[c.seg_end];
+                p->chunks.push_back(c);
+                c = sbr_plan::Chunk{c.seg_end, c.seg_end, p->seg_base[c.seg_end], 0, 0};
+            }
+            p->segs[g].zbase = c.zcount;
+            c.zcount += px;
+            c.seg_end = (int64_t)g + 1;
+        }
+        c.item_end = p->seg_base[c.seg_end];
+        p->chunks.push_back(c);
+        for (const auto& ch : p->chunks) p->zbuf_elems = std::max(p->zbuf_elems, ch.zcount);
+    }
+
     sbr_status st;
     int64_t& b = p->device_bytes;
+    if (p->raster) {
+        if ((st = zalloc(&p->d_zbuf, (size_t)p->zbuf_elems, b)) != SBR_OK) {
+            release(p);
+            return st;
+        }
+        // empty entries are all ones; the trace kernel restores them after reading
+        cudaError_t e = cudaMemset(p->d_zbuf, 0xff, (size_t)p->zbuf_elems * sizeof(unsigned long long));
+        if (e != cudaSuccess) {
+            release(p);
+            return cuda_fail(e, "first-hit buffer init");
+        }
+    }
     if ((st = upload(&p->d_segs, p->segs, b)) != SBR_OK || (st = upload(&p->d_seg_base, p->seg_base, b)) != SBR_OK ||
         (st = upload(&p->d_jobs, p->jobs, b)) != SBR_OK || (st = upload(&p->d_freqs, p->freqs, b)) != SBR_OK ||
         (st = upload(&p->d_quantum, p->quantum, b)) != SBR_OK ||
@@ -336,7 +381,7 @@ sbr_status sbr_plan_create(sbr_scene* s, const sbr_job* jobs, size_t n_jobs, con
         (st = zalloc(&p->d_acc_stats, 4 * (size_t)p->n_segs, b)) != SBR_OK ||
         (st = zalloc(&p->d_field, 2 * (size_t)p->n_samples, b)) != SBR_OK ||
         (st = zalloc(&p->d_stats, 4 * (size_t)p->n_segs, b)) != SBR_OK ||
-        (st = zalloc(&p->d_queue, 1 + (size_t)p->n_samples, b)) != SBR_OK) {
+        (st = zalloc(&p->d_queue, 1 + (size_t)p->n_samples + p->chunks.size(), b)) != SBR_OK) {
         release(p);
         return st;
     }
@@ -419,7 +464,11 @@ sbr_status sbr_plan_info_get(const sbr_plan* p, sbr_plan_info* out) {
     out->n_rays_grid = p->n_rays_grid;
     out->n_pol = 1;
     int64_t launches = 1;
-    if (p->mode == SBR_MODE_BATCHED) launches += p->n_items > 0 ? 1 : 0;
+    if (p->mode == SBR_MODE_BATCHED && p->raster) {
+        for (const auto& ch : p->chunks) launches += 1 + (ch.item_end > ch.item_begin ? 1 : 0);
+    } else if (p->mode == SBR_MODE_BATCHED) {
+        launches += p->n_items > 0 ? 1 : 0;
+    }
     else
         for (size_t g = 0; g < p->segs.size(); ++g)
             if (p->seg_base[g + 1] > p->seg_base[g]) launches += p->jobs[p->segs[g].job].n_freqs;

@@ -20,7 +20,7 @@ struct sbr_scene {
     std::vector<uint32_t> idx;
     std::vector<int32_t> order;      // leaf slot -> caller triangle index
     // device
-    sbr::GNode* d_nodes = nullptr;
+    sbr::GNode4* d_nodes = nullptr;
     int64_t n_gnodes = 0;
     int64_t n_bin_nodes = 0;
     sbr::GTri* d_tris = nullptr;
@@ -73,6 +73,16 @@ struct sbr_plan {
     uint32_t* d_err = nullptr;
     const volatile int32_t* d_cancel = nullptr;
     int64_t device_bytes = 0;
+
+    // first-hit rasterisation: segments are processed in chunks whose first-hit
+    // buffers fit `d_zbuf`; each chunk = raster launch + trace launch
+    struct Chunk {
+        int64_t seg_begin, seg_end, item_begin, item_end, zcount;
+    };
+    bool raster = false;
+    std::vector<Chunk> chunks;
+    unsigned long long* d_zbuf = nullptr;
+    int64_t zbuf_elems = 0;
 
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaGraphExec_t graph = nullptr;

@@ -152,35 +152,74 @@ sbr_status sbr_scene_create(const float* xyz, size_t nverts, const uint32_t* tri
     s->depth = tree.depth;
     for (int a = 0; a < 3; ++a) { s->aabb_lo[a] = tree.nodes[0].lo[a]; s->aabb_hi[a] = tree.nodes[0].hi[a]; }
 
-    // GPU nodes: inner binary nodes in pre-order, both child boxes per node
-    std::vector<GNode> g;
+    // GPU nodes: the binary tree collapsed to 4-wide nodes.  A 4-wide node takes a
+    // binary node's two children and keeps opening its largest (by surface area)
+    // inner child until it holds four; siblings are stored contiguously, subtrees
+    // depth first.
+    std::vector<GNode4> g;
     auto leafRef = [](const BinNode& b) { return ~(b.first * 16 + b.count); };
-    const float far = 1e30f;
+    auto area = [](const BinNode& b) {
+        float d0 = b.hi[0] - b.lo[0], d1 = b.hi[1] - b.lo[1], d2 = b.hi[2] - b.lo[2];
+        return d0 * d1 + d1 * d2 + d2 * d0;
+    };
+    auto fill = [&](GNode4& n, int c, const BinNode* b, int ref) {
+        const float far = 1e30f;
+        float lo[3] = {far, far, far}, hi[3] = {far, far, far};
+        if (b) for (int a = 0; a < 3; ++a) { lo[a] = b->lo[a]; hi[a] = b->hi[a]; }
+        (&n.lox.x)[c] = lo[0]; (&n.hix.x)[c] = hi[0];
+        (&n.loy.x)[c] = lo[1]; (&n.hiy.x)[c] = hi[1];
+        (&n.loz.x)[c] = lo[2]; (&n.hiz.x)[c] = hi[2];
+        (&n.child.x)[c] = ref;
+    };
     if (tree.nodes[0].left < 0) {
-        const BinNode& r = tree.nodes[0];
-        GNode n;
-        n.a = make_float4(r.lo[0], r.hi[0], r.lo[1], r.hi[1]);
-        n.b = make_float4(far, far, far, far);
-        n.c = make_float4(r.lo[2], r.hi[2], far, far);
-        n.link = make_int4(leafRef(r), ~0, 0, 0);
+        GNode4 n;
+        fill(n, 0, &tree.nodes[0], leafRef(tree.nodes[0]));
+        for (int c = 1; c < 4; ++c) fill(n, c, nullptr, ~0);
         g.push_back(n);
     } else {
-        std::vector<int32_t> gi(tree.nodes.size(), -1);
-        int32_t c = 0;
-        for (size_t i = 0; i < tree.nodes.size(); ++i)
-            if (tree.nodes[i].left >= 0) gi[i] = c++;
-        g.resize(c);
-        for (size_t i = 0; i < tree.nodes.size(); ++i) {
-            const BinNode& p = tree.nodes[i];
-            if (p.left < 0) continue;
-            const BinNode& L = tree.nodes[p.left];
-            const BinNode& R = tree.nodes[p.right];
-            GNode n;
-            n.a = make_float4(L.lo[0], L.hi[0], L.lo[1], L.hi[1]);
-            n.b = make_float4(R.lo[0], R.hi[0], R.lo[1], R.hi[1]);
-            n.c = make_float4(L.lo[2], L.hi[2], R.lo[2], R.hi[2]);
-            n.link = make_int4(L.left >= 0 ? gi[p.left] : leafRef(L), R.left >= 0 ? gi[p.right] : leafRef(R), 0, 0);
-            g[gi[i]] = n;
+        // A walker entering a node may hold, per ancestor, one stack entry for each
+        // ancestor child it did not enter; `need` is that bound on arrival, and a node
+        // only opens children while need + (children - 1) stays within the walker's
+        // stack capacity.
+        struct Work {
+            int32_t bin, slot, need;
+        };
+        g.emplace_back();
+        std::vector<Work> work{{0, 0, 0}};
+        while (!work.empty()) {
+            const Work w = work.back();
+            const int32_t b = w.bin, slot = w.slot;
+            work.pop_back();
+            std::vector<int32_t> kids{tree.nodes[b].left, tree.nodes[b].right};
+            while (kids.size() < 4 && w.need + (int)kids.size() <= kStackDepth) {
+                int best = -1;
+                float ba = -1.0f;
+                for (size_t k = 0; k < kids.size(); ++k) {
+                    const BinNode& K = tree.nodes[kids[k]];
+                    if (K.left >= 0 && area(K) > ba) { ba = area(K); best = (int)k; }
+                }
+                if (best < 0) break;
+                const BinNode& K = tree.nodes[kids[best]];
+                kids[best] = K.left;
+                kids.insert(kids.begin() + best + 1, K.right);
+            }
+            GNode4 n;
+            std::vector<Work> inner;
+            const int32_t need = w.need + (int32_t)kids.size() - 1;
+            for (int c = 0; c < 4; ++c) {
+                if (c >= (int)kids.size()) { fill(n, c, nullptr, ~0); continue; }
+                const BinNode& K = tree.nodes[kids[c]];
+                if (K.left >= 0) {
+                    int32_t idx = (int32_t)g.size() + (int32_t)inner.size();
+                    inner.push_back({kids[c], idx, need});
+                    fill(n, c, &K, idx);
+                } else {
+                    fill(n, c, &K, leafRef(K));
+                }
+            }
+            g[slot] = n;
+            g.resize(g.size() + inner.size());
+            for (auto it = inner.rbegin(); it != inner.rend(); ++it) work.push_back(*it);
         }
     }
     s->n_gnodes = (int64_t)g.size();
@@ -216,7 +255,7 @@ sbr_status sbr_scene_create(const float* xyz, size_t nverts, const uint32_t* tri
         return st;
     };
     cudaError_t e;
-    size_t nb = sizeof(GNode) * g.size(), tb = sizeof(GTri) * tr.size(), ib = sizeof(int32_t) * ids.size();
+    size_t nb = sizeof(GNode4) * g.size(), tb = sizeof(GTri) * tr.size(), ib = sizeof(int32_t) * ids.size();
     if ((e = cudaMalloc(&s->d_nodes, nb)) != cudaSuccess || (e = cudaMalloc(&s->d_tris, tb)) != cudaSuccess ||
         (e = cudaMalloc(&s->d_tri_id, ib)) != cudaSuccess || (e = cudaMalloc(&s->d_err, sizeof(uint32_t))) != cudaSuccess)
         return bail(fail(SBR_ERR_OOM, std::string("device allocation failed: ") + cudaGetErrorString(e)));

@@ -42,6 +42,7 @@ struct TraceParams {
     uint32_t* err;
     const volatile int32_t* cancel;
     sbr_ray_record* records;       // debug records (REC instantiation only)
+    unsigned long long* zbuf;      // first-hit buffer of the launch's chunk, or null (walk the BVH)
 };
 
 constexpr int kMaxK = 128;   // frequencies per job
@@ -56,6 +57,7 @@ struct RayF {
     double L;       // FP64 path (mixed)
     float dist32;   // FP32 path (reference FP32 arithmetic)
     int count;
+    int zidx;       // entry of this ray in the first-hit buffer
 };
 struct RayD {
     D3 o, d, nl, dl;
@@ -73,21 +75,28 @@ struct RayOut {
 };
 
 // ------------------------------------------------------------ FP32 / mixed
+// Origin of the primary ray of pixel (i, j) (src/cuda/rtKernels.cu:120-123); the
+// trace and the first-hit raster both use this, so they test identical rays.
 template <int PREC>
-__device__ __forceinline__ void start_f(RayF& r, const Segment& G, const JobConst& J, int i, int j) {
+__device__ __forceinline__ F3 primary_origin(const Segment& G, const JobConst& J, int i, int j) {
     if (PREC == SBR_PREC_FP32) {
         const float u = __fdiv_rn(float(i) + 0.5f, float(J.nx));
         const float v = __fdiv_rn(float(j) + 0.5f, float(J.ny));
-        r.o = f3(G.llcf[0] + u * G.uf[0] + v * G.vf[0], G.llcf[1] + u * G.uf[1] + v * G.vf[1],
-                 G.llcf[2] + u * G.uf[2] + v * G.vf[2]);
-        r.L = 0.0;
+        return f3(G.llcf[0] + u * G.uf[0] + v * G.vf[0], G.llcf[1] + u * G.uf[1] + v * G.vf[1],
+                  G.llcf[2] + u * G.uf[2] + v * G.vf[2]);
     } else {
         const double u = (double(i) + 0.5) * J.inv_nx;
         const double v = (double(j) + 0.5) * J.inv_ny;
-        r.o = f3(float(G.llc[0] + u * G.u[0] + v * G.v[0]), float(G.llc[1] + u * G.u[1] + v * G.v[1]),
-                 float(G.llc[2] + u * G.u[2] + v * G.v[2]));
-        r.L = G.shift;
+        return f3(float(G.llc[0] + u * G.u[0] + v * G.v[0]), float(G.llc[1] + u * G.u[1] + v * G.v[1]),
+                  float(G.llc[2] + u * G.u[2] + v * G.v[2]));
     }
+}
+
+template <int PREC>
+__device__ __forceinline__ void start_f(RayF& r, const Segment& G, const JobConst& J, int i, int j) {
+    r.o = primary_origin<PREC>(G, J, i, j);
+    r.L = PREC == SBR_PREC_FP32 ? 0.0 : G.shift;
+    r.zidx = (int)(G.zbase + (int64_t)(j - G.j0) * G.ni + (i - G.i0));
     r.d = f3(G.rdf[0], G.rdf[1], G.rdf[2]);
     r.nl = f3(0, 0, 0);
     r.dl = f3(0, 0, 0);
@@ -96,10 +105,22 @@ __device__ __forceinline__ void start_f(RayF& r, const Segment& G, const JobCons
 }
 
 // One closest-hit query, then reflect and nudge; true when the ray is finished.
+// The first query is read from the first-hit buffer when there is one (and the
+// entry is restored to empty for the next chunk).
 template <int PREC, bool REC>
-__device__ __forceinline__ bool step_f(RayF& r, const SceneView& S, int maxB, uint32_t& err, sbr_ray_record* rec) {
+__device__ __forceinline__ bool step_f(RayF& r, const SceneView& S, int maxB, uint32_t& err, sbr_ray_record* rec,
+                                       unsigned long long* zbuf) {
     float tB = 1e20f;
-    const int slot = Walker<false>::closest(S, r.o, r.d, 1.0e-3f, tB, err);
+    int slot;
+    if (zbuf != nullptr && r.count == 0) {
+        const unsigned long long key = zbuf[r.zidx];
+        zbuf[r.zidx] = ~0ull;
+        if (key == ~0ull) return true;
+        tB = __uint_as_float((unsigned)(key >> 32));
+        slot = (int)(unsigned)key;
+    } else {
+        slot = Walker<false>::closest(S, r.o, r.d, 1.0e-3f, tB, err);
+    }
     if (slot < 0) return true;
     const GTri* T = S.tris + slot;
     const F3 n = f3(__ldg(&T->p.w), __ldg(&T->e1.w), __ldg(&T->e2.w));
@@ -314,7 +335,7 @@ __global__ void __launch_bounds__(kCtaThreads, kMinCtasPerSm) k_trace(const Trac
             out.amp = 0.0f;
             if (active) {
                 done = F64 ? step_d<REC>(rd, P.S, J.max_bounces, err, rec)
-                           : step_f<PREC, REC>(rf, P.S, J.max_bounces, err, rec);
+                           : step_f<PREC, REC>(rf, P.S, J.max_bounces, err, rec, P.zbuf);
                 ++queries;
                 if (done) {
                     const int cnt = F64 ? rd.count : rf.count;
@@ -414,6 +435,90 @@ __global__ void __launch_bounds__(kCtaThreads, kMinCtasPerSm) k_trace(const Trac
         }
     }
     if (err) atomicOr(P.err, err);
+}
+
+// ------------------------------------------------------- first-hit raster
+struct RasterParams {
+    SceneView S;
+    const Segment* segs;
+    const JobConst* jobs;
+    int64_t seg_begin;        // first segment of the chunk (blockIdx.y counts from here)
+    int32_t ntris;
+    unsigned long long* zbuf; // [chunk pixels]: (float bits of t) << 32 | triangle slot, all ones = empty
+};
+
+constexpr float kRasterMargin = 0.05f;  // pixels; covers FP32 rounding of ray origins and barycentrics
+
+template <int PREC>
+__device__ __forceinline__ void raster_pixel(const GTri& T, int slot, const Segment& G, const JobConst& J, F3 d,
+                                             int i, int j, unsigned long long* zbuf) {
+    const F3 o = primary_origin<PREC>(G, J, i, j);
+    float t;
+    if (mt_f(T, o, d, 1.0e-3f, 1e20f, t)) {
+        const unsigned long long key = ((unsigned long long)__float_as_uint(t) << 32) | (unsigned)slot;
+        atomicMin(zbuf + G.zbase + (int64_t)(j - G.j0) * G.ni + (i - G.i0), key);
+    }
+}
+
+// First closest hit of every primary ray of a chunk of segments.  Primary rays of
+// one angle are parallel and start at the pixel centres of the launcher grid, so a
+// triangle can only be hit by the rays whose pixel centres lie inside its projected
+// box (plus a small margin).  Each (segment, triangle) pair tests exactly those
+// rays with the trace's own Moller-Trumbore and keeps, per pixel, the nearest hit
+// (smallest t, then smallest slot) with a 64-bit atomicMin.  Triangles covering
+// few pixels are done by one lane; larger ones are spread over the warp.
+template <int PREC>
+__global__ void __launch_bounds__(256) k_raster(const RasterParams R) {
+    constexpr unsigned FULL = 0xffffffffu;
+    const Segment& G = R.segs[R.seg_begin + blockIdx.y];
+    if (G.ni <= 0 || G.nj <= 0) return;
+    const JobConst J = R.jobs[G.job];
+    const F3 d = f3(G.rdf[0], G.rdf[1], G.rdf[2]);
+    const int lane = threadIdx.x & 31;
+    const int i_last = G.i0 + G.ni - 1, j_last = G.j0 + G.nj - 1;
+    for (int base = blockIdx.x * blockDim.x; base < R.ntris; base += gridDim.x * blockDim.x) {
+        const int slot = base + threadIdx.x;
+        int ilo = 1, ihi = 0, jlo = 1, jhi = 0;
+        GTri T;
+        if (slot < R.ntris) {
+            T = R.S.tris[slot];
+            // the triangle Moller-Trumbore sees: v0, v0 + e1, v0 + e2 (exact in FP64)
+            const double x0 = T.p.x, y0 = T.p.y, z0 = T.p.z;
+            const double X[3] = {x0, x0 + T.e1.x, x0 + T.e2.x};
+            const double Y[3] = {y0, y0 + T.e1.y, y0 + T.e2.y};
+            const double Z[3] = {z0, z0 + T.e1.z, z0 + T.e2.z};
+            double smin = 1e300, smax = -1e300, tmin = 1e300, tmax = -1e300;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const double s = G.ps[0] * X[k] + G.ps[1] * Y[k] + G.ps[2] * Z[k] + G.ps[3];
+                const double t = G.pt[0] * X[k] + G.pt[1] * Y[k] + G.pt[2] * Z[k] + G.pt[3];
+                smin = fmin(smin, s); smax = fmax(smax, s);
+                tmin = fmin(tmin, t); tmax = fmax(tmax, t);
+            }
+            ilo = max(G.i0, (int)fmax(ceil(smin - kRasterMargin), -1.0));
+            ihi = min(i_last, (int)fmin(floor(smax + kRasterMargin), 2.0e9));
+            jlo = max(G.j0, (int)fmax(ceil(tmin - kRasterMargin), -1.0));
+            jhi = min(j_last, (int)fmin(floor(tmax + kRasterMargin), 2.0e9));
+        }
+        const int w = ihi - ilo + 1;
+        const int cnt = (ihi >= ilo && jhi >= jlo) ? w * (jhi - jlo + 1) : 0;
+        const bool big = cnt > 32;
+        if (!big) {
+            for (int jj = jlo; jj <= jhi; ++jj)
+                for (int ii = ilo; ii <= ihi; ++ii) raster_pixel<PREC>(T, slot, G, J, d, ii, jj, R.zbuf);
+        }
+        unsigned m = __ballot_sync(FULL, big);
+        while (m) {
+            const int src = __ffs(m) - 1;
+            m &= m - 1;
+            const int s_slot = __shfl_sync(FULL, slot, src);
+            const int s_ilo = __shfl_sync(FULL, ilo, src), s_jlo = __shfl_sync(FULL, jlo, src);
+            const int s_w = __shfl_sync(FULL, w, src), s_cnt = __shfl_sync(FULL, cnt, src);
+            const GTri Ts = R.S.tris[s_slot];
+            for (int c = lane; c < s_cnt; c += 32)
+                raster_pixel<PREC>(Ts, s_slot, G, J, d, s_ilo + c % s_w, s_jlo + c / s_w, R.zbuf);
+        }
+    }
 }
 
 // Converts the fixed-point accumulators (summing the replicas exactly, as
@@ -524,7 +629,38 @@ sbr_status plan_launch(sbr_plan* pl, bool records, sbr_ray_record* d_records) {
             sbr_status s = resident_ctas(fn, pl->ctas_per_sm, pl->num_sms, &pl->persistent_grid);
             if (s != SBR_OK) return s;
         }
-        if (pl->mode == SBR_MODE_BATCHED || records) {
+        if ((pl->mode == SBR_MODE_BATCHED || records) && pl->raster) {
+            // per chunk of segments: first hits by raster, then the persistent trace
+            const void* rfn = pl->prec == SBR_PREC_FP32 ? reinterpret_cast<const void*>(&k_raster<SBR_PREC_FP32>)
+                                                        : reinterpret_cast<const void*>(&k_raster<SBR_PREC_MIXED>);
+            p.k_begin = 0;
+            p.k_count = 0;
+            p.count_stats = 1;
+            p.zbuf = pl->d_zbuf;
+            for (size_t c = 0; c < pl->chunks.size(); ++c) {
+                const sbr_plan::Chunk& ch = pl->chunks[c];
+                RasterParams r{};
+                r.S = pl->scene_view;
+                r.segs = pl->d_segs;
+                r.jobs = pl->d_jobs;
+                r.seg_begin = ch.seg_begin;
+                r.ntris = (int32_t)pl->scene->ntris;
+                r.zbuf = pl->d_zbuf;
+                void* rargs[] = {&r};
+                const unsigned gx = (unsigned)std::min<long long>((pl->scene->ntris + 255) / 256, 4096);
+                SBR_CUDA(cudaLaunchKernel(rfn, dim3(gx, (unsigned)(ch.seg_end - ch.seg_begin)), dim3(256), rargs, 0, st));
+                ++launches;
+                if (ch.item_end > ch.item_begin) {
+                    p.item_begin = ch.item_begin;
+                    p.item_end = ch.item_end;
+                    p.queue = pl->d_queue + 1 + pl->n_samples + c;
+                    const int grid = (int)std::min<long long>(pl->persistent_grid, (ch.item_end - ch.item_begin + 3) / 4);
+                    sbr_status s = launch_trace(fn, grid, st, p);
+                    if (s != SBR_OK) return s;
+                    ++launches;
+                }
+            }
+        } else if (pl->mode == SBR_MODE_BATCHED || records) {
             p.k_begin = 0;
             p.k_count = 0;
             p.count_stats = 1;
@@ -560,7 +696,7 @@ sbr_status plan_launch(sbr_plan* pl, bool records, sbr_ray_record* d_records) {
         }
     }
     finalize(pl->n_samples, kAccReplicas, pl->d_quantum, pl->d_acc, pl->d_field, (long long)pl->n_segs * 4,
-             pl->d_acc_stats, pl->d_stats, pl->d_queue, pl->n_samples + 1, st);
+             pl->d_acc_stats, pl->d_stats, pl->d_queue, pl->n_samples + 1 + (long long)pl->chunks.size(), st);
     SBR_CUDA(cudaGetLastError());
     ++launches;
     pl->launches = launches;

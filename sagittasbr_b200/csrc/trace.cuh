@@ -1,5 +1,5 @@
 // trace.cuh -- device building blocks of the SBR path for sm_100a:
-// closest-hit traversal of the GNode BVH, the bounce loop with PEC reflection and
+// closest-hit traversal of the 4-wide BVH, the bounce loop with PEC reflection and
 // the reference's scalar PO exit-ray term.
 //
 // Semantics follow the reference per-ray routine:
@@ -11,7 +11,7 @@
 //   PO: R^n, cos = n.(-d_last) > 0, phase 2 k L, mag = k A / (4 pi) * 2 cos R^n,
 //       term (-mag sin, mag cos) ............... src/cuda/poKernels.cu:81-109
 // The traversal order differs from the reference (nearest child first, entries
-// beyond the current closest hit are skipped, 2-wide nodes); it returns the same
+// beyond the current closest hit are skipped, 4-wide nodes); it returns the same
 // closest hit except for exact ties between triangles (shared edges), where the
 // reference keeps the last triangle tested.
 #pragma once
@@ -138,13 +138,37 @@ __device__ __forceinline__ bool mt_d(const GTri64& T, D3 o, D3 d, double tMin, d
     return true;
 }
 
-__device__ __forceinline__ GNode load_node(const GNode* p) {
-    GNode n;
-    n.a = __ldg(&p->a);
-    n.b = __ldg(&p->b);
-    n.c = __ldg(&p->c);
-    n.link = __ldg(&p->link);
+__device__ __forceinline__ GNode4 load_node(const GNode4* p) {
+    GNode4 n;
+    n.lox = __ldg(&p->lox);
+    n.hix = __ldg(&p->hix);
+    n.loy = __ldg(&p->loy);
+    n.hiy = __ldg(&p->hiy);
+    n.loz = __ldg(&p->loz);
+    n.hiz = __ldg(&p->hiz);
+    n.child = __ldg(&p->child);
     return n;
+}
+
+// Sorts four (entry distance, child) pairs by distance, nearest first (five
+// compare-exchanges, no branches; misses carry +inf and end up last).
+template <typename T>
+__device__ __forceinline__ void cswap(T& ta, int& ca, T& tb, int& cb) {
+    const bool s = tb < ta;
+    const T t = s ? tb : ta;
+    tb = s ? ta : tb;
+    ta = t;
+    const int c = s ? cb : ca;
+    cb = s ? ca : cb;
+    ca = c;
+}
+template <typename T>
+__device__ __forceinline__ void sort4(T (&t)[4], int (&c)[4]) {
+    cswap(t[0], c[0], t[1], c[1]);
+    cswap(t[2], c[2], t[3], c[3]);
+    cswap(t[0], c[0], t[2], c[2]);
+    cswap(t[1], c[1], t[3], c[3]);
+    cswap(t[1], c[1], t[2], c[2]);
 }
 
 constexpr uint32_t kIterBudget = 1u << 22;  // node + leaf steps per query before giving up
@@ -156,10 +180,11 @@ __device__ __forceinline__ unsigned long long pack_entry(int ref, float t) {
 }
 
 // Closest hit along o + t d with t in [tMin, tBest]: returns the leaf slot of the hit
-// triangle (or -1) and lowers tBest to its distance.  While-while structure:
-// inner nodes are walked (nearer child first, farther child pushed with its entry
-// distance) until a leaf is reached, leaves are tested, popped entries beyond the
-// current hit are skipped.  `err` collects DEV_ERR_* bits.
+// triangle (or -1) and lowers tBest to its distance.  While-while structure over
+// 4-wide nodes: the children a ray's slab test accepts are ordered by entry
+// distance, the nearest is entered and the others are pushed (farthest first) with
+// their entry distances; leaves are tested, popped entries beyond the current hit
+// are skipped.  `err` collects DEV_ERR_* bits.
 template <bool kF64>
 struct Walker;
 
@@ -174,27 +199,34 @@ struct Walker<false> {
         int ref = 0;
         int best = -1;
         uint32_t iters = 0;
+        auto push = [&](int r, float t) {
+            if (sp < kStackDepth) stack[sp++] = pack_entry(r, t);
+            else err |= DEV_ERR_STACK;
+        };
+        auto pop = [&]() {
+            while (sp > 0) {
+                const unsigned long long e = stack[--sp];
+                if (__uint_as_float((unsigned)(e >> 32)) <= tBest) { ref = (int)(unsigned)e; return true; }
+            }
+            return false;
+        };
         for (;;) {
             while (ref >= 0) {
                 if (++iters > kIterBudget) { err |= DEV_ERR_BUDGET; return -1; }
-                const GNode n = load_node(S.nodes + ref);
-                const float t0 = slab_f(n.a.x, n.a.y, n.a.z, n.a.w, n.c.x, n.c.y, inv, oi, tMin, tBest);
-                const float t1 = slab_f(n.b.x, n.b.y, n.b.z, n.b.w, n.c.z, n.c.w, inv, oi, tMin, tBest);
-                const bool h0 = t0 <= tBest, h1 = t1 <= tBest;
-                if (h0 && h1) {
-                    const bool f = t1 < t0;
-                    if (sp < kStackDepth) stack[sp++] = pack_entry(f ? n.link.x : n.link.y, f ? t0 : t1);
-                    else err |= DEV_ERR_STACK;
-                    ref = f ? n.link.y : n.link.x;
-                } else if (h0 || h1) {
-                    ref = h0 ? n.link.x : n.link.y;
-                } else {
-                    bool found = false;
-                    while (sp > 0) {
-                        const unsigned long long e = stack[--sp];
-                        if (__uint_as_float((unsigned)(e >> 32)) <= tBest) { ref = (int)(unsigned)e; found = true; break; }
-                    }
-                    if (!found) return best;
+                const GNode4 n = load_node(S.nodes + ref);
+                float t[4] = {slab_f(n.lox.x, n.hix.x, n.loy.x, n.hiy.x, n.loz.x, n.hiz.x, inv, oi, tMin, tBest),
+                              slab_f(n.lox.y, n.hix.y, n.loy.y, n.hiy.y, n.loz.y, n.hiz.y, inv, oi, tMin, tBest),
+                              slab_f(n.lox.z, n.hix.z, n.loy.z, n.hiy.z, n.loz.z, n.hiz.z, inv, oi, tMin, tBest),
+                              slab_f(n.lox.w, n.hix.w, n.loy.w, n.hiy.w, n.loz.w, n.hiz.w, inv, oi, tMin, tBest)};
+                int c[4] = {n.child.x, n.child.y, n.child.z, n.child.w};
+                sort4(t, c);
+                if (t[0] <= tBest) {
+                    if (t[3] <= tBest) push(c[3], t[3]);
+                    if (t[2] <= tBest) push(c[2], t[2]);
+                    if (t[1] <= tBest) push(c[1], t[1]);
+                    ref = c[0];
+                } else if (!pop()) {
+                    return best;
                 }
             }
             do {
@@ -202,15 +234,10 @@ struct Walker<false> {
                 const int code = ~ref;
                 const int first = code >> 4, cnt = code & 15;
                 for (int k = 0; k < cnt; ++k) {
-                    float t;
-                    if (mt_f(S.tris[first + k], o, d, tMin, tBest, t)) { tBest = t; best = first + k; }
+                    float tt;
+                    if (mt_f(S.tris[first + k], o, d, tMin, tBest, tt)) { tBest = tt; best = first + k; }
                 }
-                bool found = false;
-                while (sp > 0) {
-                    const unsigned long long e = stack[--sp];
-                    if (__uint_as_float((unsigned)(e >> 32)) <= tBest) { ref = (int)(unsigned)e; found = true; break; }
-                }
-                if (!found) return best;
+                if (!pop()) return best;
             } while (ref < 0);
         }
     }
@@ -228,28 +255,34 @@ struct Walker<true> {
         uint32_t iters = 0;
         // entry distances are stored rounded down to float, so the pruning test
         // (entry <= tBest) stays conservative
-        auto down = [](double t) { return __double2float_rd(t); };
+        auto push = [&](int r, double t) {
+            if (sp < kStackDepth) stack[sp++] = pack_entry(r, __double2float_rd(t));
+            else err |= DEV_ERR_STACK;
+        };
+        auto pop = [&]() {
+            while (sp > 0) {
+                const unsigned long long e = stack[--sp];
+                if (double(__uint_as_float((unsigned)(e >> 32))) <= tBest) { ref = (int)(unsigned)e; return true; }
+            }
+            return false;
+        };
         for (;;) {
             while (ref >= 0) {
                 if (++iters > kIterBudget) { err |= DEV_ERR_BUDGET; return -1; }
-                const GNode n = load_node(S.nodes + ref);
-                const double t0 = slab_d(n.a.x, n.a.y, n.a.z, n.a.w, n.c.x, n.c.y, o, inv, tMin, tBest);
-                const double t1 = slab_d(n.b.x, n.b.y, n.b.z, n.b.w, n.c.z, n.c.w, o, inv, tMin, tBest);
-                const bool h0 = t0 <= tBest, h1 = t1 <= tBest;
-                if (h0 && h1) {
-                    const bool f = t1 < t0;
-                    if (sp < kStackDepth) stack[sp++] = pack_entry(f ? n.link.x : n.link.y, down(f ? t0 : t1));
-                    else err |= DEV_ERR_STACK;
-                    ref = f ? n.link.y : n.link.x;
-                } else if (h0 || h1) {
-                    ref = h0 ? n.link.x : n.link.y;
-                } else {
-                    bool found = false;
-                    while (sp > 0) {
-                        const unsigned long long e = stack[--sp];
-                        if (double(__uint_as_float((unsigned)(e >> 32))) <= tBest) { ref = (int)(unsigned)e; found = true; break; }
-                    }
-                    if (!found) return best;
+                const GNode4 n = load_node(S.nodes + ref);
+                double t[4] = {slab_d(n.lox.x, n.hix.x, n.loy.x, n.hiy.x, n.loz.x, n.hiz.x, o, inv, tMin, tBest),
+                               slab_d(n.lox.y, n.hix.y, n.loy.y, n.hiy.y, n.loz.y, n.hiz.y, o, inv, tMin, tBest),
+                               slab_d(n.lox.z, n.hix.z, n.loy.z, n.hiy.z, n.loz.z, n.hiz.z, o, inv, tMin, tBest),
+                               slab_d(n.lox.w, n.hix.w, n.loy.w, n.hiy.w, n.loz.w, n.hiz.w, o, inv, tMin, tBest)};
+                int c[4] = {n.child.x, n.child.y, n.child.z, n.child.w};
+                sort4(t, c);
+                if (t[0] <= tBest) {
+                    if (t[3] <= tBest) push(c[3], t[3]);
+                    if (t[2] <= tBest) push(c[2], t[2]);
+                    if (t[1] <= tBest) push(c[1], t[1]);
+                    ref = c[0];
+                } else if (!pop()) {
+                    return best;
                 }
             }
             do {
@@ -257,15 +290,10 @@ struct Walker<true> {
                 const int code = ~ref;
                 const int first = code >> 4, cnt = code & 15;
                 for (int k = 0; k < cnt; ++k) {
-                    double t;
-                    if (mt_d(S.tris64[first + k], o, d, tMin, tBest, t)) { tBest = t; best = first + k; }
+                    double tt;
+                    if (mt_d(S.tris64[first + k], o, d, tMin, tBest, tt)) { tBest = tt; best = first + k; }
                 }
-                bool found = false;
-                while (sp > 0) {
-                    const unsigned long long e = stack[--sp];
-                    if (double(__uint_as_float((unsigned)(e >> 32))) <= tBest) { ref = (int)(unsigned)e; found = true; break; }
-                }
-                if (!found) return best;
+                if (!pop()) return best;
             } while (ref < 0);
         }
     }

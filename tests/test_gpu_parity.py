@@ -102,6 +102,28 @@ def test_hit_sequences(brute, name, prec):
 
 
 @pytest.mark.parametrize("name", sorted(CASES))
+def test_first_hit_raster_matches_walk(golden, brute, name):
+    """The opt-in first-hit raster gives the same hit sequences (unambiguous rays)
+    and fields as the BVH walk, in FP32 and mixed precision."""
+    v, t, th, ph, fr, nx, ny, G, mb, R = CASES[name]
+    job = sbr.JobSpec(th, ph, fr, nx, ny, G, mb, R)
+    o = brute[name].rays
+    ok = o["amb"] == 0
+    with sbr.Scene(v, t) as sc:
+        for prec in (sbr.PREC_MIXED, sbr.PREC_FP32):
+            rec = sbr.trace_records(sc, job, precision=prec, first_hit=sbr.FIRST_HIT_RASTER)
+            walk = sbr.trace_records(sc, job, precision=prec, first_hit=sbr.FIRST_HIT_TRAVERSE)
+            np.testing.assert_array_equal(rec["count"][ok], walk["count"][ok])
+            np.testing.assert_array_equal(rec["tri"][ok], walk["tri"][ok])
+            np.testing.assert_array_equal(rec["dist"][ok], walk["dist"][ok])
+            if prec == sbr.PREC_MIXED:
+                np.testing.assert_array_equal(rec["tri"][ok], o["tri"][ok])
+            res = sbr.run(sc, job, precision=prec, first_hit=sbr.FIRST_HIT_RASTER)
+            bound = field_bound(brute[name], fr, G, nx, ny, R, mb, prec)
+            assert np.all(np.abs(res.field.reshape(len(th), len(fr)) - golden[f"{name}/field"]) <= bound)
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
 def test_reference_hit_counts(golden, brute, name):
     """GPU FP64 hit counts and paths against the reference's own per-ray output."""
     v, t, th, ph, fr, nx, ny, G, mb, R = CASES[name]
