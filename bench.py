@@ -250,6 +250,8 @@ def main():
                     help="per-angle mode is timed on every n-th angle of the sweep")
     ap.add_argument("--first-hit", default="traverse", choices=["traverse", "raster"],
                     help="first closest hit by BVH walk (default) or by the first-hit raster")
+    ap.add_argument("--polarization", default="scalar", choices=["scalar", "hhvv"],
+                    help="the reference's scalar PO term, or HH and VV fields with E-vector tracking")
     ap.add_argument("--fp64-check", type=int, default=0,
                     help="compare with a full-FP64 run of the batched job on this many angles")
     args = ap.parse_args()
@@ -282,7 +284,9 @@ def main():
     scene_s = time.perf_counter() - t_scene
     job = sbr.JobSpec(w["theta"], w["phi"], w["freqs"], w["nx"], w["ny"], w["G"], w["max_bounces"], w["R"])
     first_hit = sbr.FIRST_HIT_RASTER if args.first_hit == "raster" else sbr.FIRST_HIT_TRAVERSE
-    plan = sbr.Plan(scene, [job], mode=sbr.MODE_BATCHED, precision=sbr.PREC_MIXED, stream=sp, first_hit=first_hit)
+    pol = sbr.POL_HHVV if args.polarization == "hhvv" else sbr.POL_SCALAR
+    plan = sbr.Plan(scene, [job], mode=sbr.MODE_BATCHED, precision=sbr.PREC_MIXED, stream=sp, first_hit=first_hit,
+                    polarization=pol)
     info = plan.info
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
@@ -327,7 +331,8 @@ def main():
     for s in range(1 + min(args.steps, 3)):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        r2 = sbr.run(scene, job, mode=sbr.MODE_BATCHED, precision=sbr.PREC_MIXED, first_hit=first_hit)
+        r2 = sbr.run(scene, job, mode=sbr.MODE_BATCHED, precision=sbr.PREC_MIXED, first_hit=first_hit,
+                     polarization=pol)
         if s:
             e2e_ms.append((time.perf_counter() - t0) * 1e3)
     e2e_t = torch.tensor([float(np.mean(e2e_ms))], device="cuda", dtype=torch.float64)
@@ -422,7 +427,7 @@ def main():
         "config": {"workload": w["name"], "angles": int(w["theta"].size), "freqs": len(w["freqs"]),
                    "triangles": int(w["tris"].shape[0]), "rays_per_angle": w["nx"] * w["ny"],
                    "rays_launched_per_step": info["n_rays_clipped"], "max_bounces": w["max_bounces"],
-                   "mode": "batched persistent", "precision": "mixed",
+                   "mode": "batched persistent", "precision": "mixed", "polarization": args.polarization,
                    "l2": "flushed before every step (256 MiB write inside the timed region)",
                    "parallelism": f"{ws} GPU(s), independent sweeps", "scene_build_s": scene_s},
         "mray_bounces_per_s": bounces_step * ws / (step_ms * 1e-3) / 1e6,

@@ -124,8 +124,18 @@ typedef struct sbr_job {
 #define SBR_FIRST_HIT_TRAVERSE 0  /* walk the BVH for every query (default) */
 #define SBR_FIRST_HIT_RASTER 1    /* first hits from the orthographic first-hit raster */
 
-#define SBR_POL_SCALAR 0      /* the reference's scalar PO term (HH == VV) */
-#define SBR_POL_HHVV 1        /* PEC E-vector tracking; fields for HH and VV */
+/* Polarisation.  SCALAR is the reference's PO term (poKernels.cu:81-109; HH == VV).
+ * HHVV (no counterpart in the reference; SBR_PREC_MIXED or SBR_PREC_FP64, at most
+ * 64 frequencies per job) tracks the HH (phi-hat) and VV (theta-hat) incident
+ * fields through every PEC reflection, E <- 2 (n.E) n - E, and gives each exit
+ * ray the scalar gate (cos = n.(-d_last) > 0) with the co-polarised amplitude
+ * 2 R^n e.(n x (d_last x E_last)) -- the PO surface current on the last surface
+ * projected on the receive polarisation, equal to the scalar 2 cos R^n for a
+ * single bounce -- and the physical path launch plane -> exit point -> launch
+ * plane instead of the scalar term's 2 * path (so multi-bounce returns add in
+ * phase).  Fields come per (sample, HH / VV). */
+#define SBR_POL_SCALAR 0
+#define SBR_POL_HHVV 1
 
 typedef struct sbr_run_opts {
     int32_t mode;             /* SBR_MODE_* */

@@ -89,6 +89,13 @@ def lib():
             _I32, _I32, _I32, _P, _P,
             _P, _P, _D, _D, _D,
         ]
+        L.oracle_sweep_pol.restype = C.c_int
+        L.oracle_sweep_pol.argtypes = [
+            _P, _I64, _P, _I64, _D,
+            _P, _P, _I64, _P, _I64,
+            _I32, _I32, _D, _I32, _D,
+            _I32, _I32, _P, _P,
+        ]
         L.oracle_build_tree.restype = _I64
         L.oracle_build_tree.argtypes = [_P, _I64, _P, _I64, _D, _P, _P, _P]
         L.oracle_frame.restype = None
@@ -168,6 +175,28 @@ def sweep(verts, tris, theta_deg, phi_deg, freqs_hz, nx, ny, grid_size, max_boun
     if rc != 0:
         raise RuntimeError(f"oracle_sweep failed with code {rc}")
     return SweepOut((re + 1j * im).reshape(na, nf), counts, rays)
+
+
+def sweep_pol(verts, tris, theta_deg, phi_deg, freqs_hz, nx, ny, grid_size, max_bounces,
+              reflection_const=1.0, accel="tree", threads=0, model_scale=1.0) -> np.ndarray:
+    """Polarised FP64 sweep (E-vector tracking, physical exit path; no reference
+    counterpart): complex128 [n_angles, n_freqs, 2] with (HH, VV) last."""
+    v, t = _mesh_args(verts, tris)
+    th = np.ascontiguousarray(theta_deg, dtype=np.float64).ravel()
+    ph = np.ascontiguousarray(phi_deg, dtype=np.float64).ravel()
+    fr = np.ascontiguousarray(np.atleast_1d(freqs_hz), dtype=np.float64)
+    na, nf = th.size, fr.size
+    re = np.zeros(na * nf * 2)
+    im = np.zeros(na * nf * 2)
+    rc = lib().oracle_sweep_pol(
+        _ptr(v), v.shape[0], _ptr(t), t.shape[0], float(model_scale),
+        _ptr(th), _ptr(ph), na, _ptr(fr), nf,
+        int(nx), int(ny), float(grid_size), int(max_bounces), float(reflection_const),
+        1 if accel == "tree" else 0, int(threads), _ptr(re), _ptr(im),
+    )
+    if rc != 0:
+        raise RuntimeError(f"oracle_sweep_pol failed with code {rc}")
+    return (re + 1j * im).reshape(na, nf, 2)
 
 
 def ref_sweep(verts, tris, theta_deg, phi_deg, freqs_hz, nx, ny, grid_size, max_bounces,

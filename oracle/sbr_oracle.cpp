@@ -517,9 +517,123 @@ int sweep_impl(const float* xyz, int64_t nverts, const uint32_t* idx, int64_t nt
     return 0;
 }
 
+// Polarised variant (no counterpart in the reference, whose PO term is scalar):
+// the same rays and hits in FP64, with the HH and VV incident fields tracked
+// through every PEC reflection (E <- 2 (n.E) n - E) and, per exit ray that the
+// scalar gate keeps (hit, cos(theta) = n.(-d_last) > 0), the co-polarised term
+//   amplitude  2 R^n e.(n x (d_last x E_last))      (e = phi-hat for HH, theta-hat for VV)
+//   path       dist + (s.llc - s.p_last)             (launch plane -> exit point -> plane)
+//   term       k A / (4 pi) * amplitude * (-sin(k path), cos(k path)).
+// Output: out[(a * nFreqs + f) * 2 + p] (p = 0 HH, 1 VV).
+int sweep_pol_impl(const float* xyz, int64_t nverts, const uint32_t* idx, int64_t ntris, double modelScale,
+                   const double* thetaDeg, const double* phiDeg, int64_t nAngles, const double* freqHz,
+                   int64_t nFreqs, int32_t nx, int32_t ny, double gridSize, int32_t maxBounces, double reflConst,
+                   int32_t accel, int32_t nThreads, double* outRe, double* outIm) {
+    typedef double R;
+    if (ntris <= 0 || nverts <= 0 || nx <= 0 || ny <= 0 || nAngles < 0 || nFreqs <= 0) return 1;
+    std::vector<Tri<R>> tris(ntris);
+    for (int64_t i = 0; i < ntris; ++i) {
+        uint32_t a = idx[3 * i], b = idx[3 * i + 1], c = idx[3 * i + 2];
+        if (a >= nverts || b >= nverts || c >= nverts) return 2;
+        auto P = [&](uint32_t k) {
+            return V3<R>(R(xyz[3 * k]) * modelScale, R(xyz[3 * k + 1]) * modelScale, R(xyz[3 * k + 2]) * modelScale);
+        };
+        tris[i] = Tri<R>{P(a), P(b), P(c), (int32_t)i};
+    }
+    std::vector<Tri<R>> original = tris;
+    TreeBuilder<R> tb(tris);
+    if (accel == 1) tb.run();
+#ifdef _OPENMP
+    if (nThreads > 0) omp_set_num_threads(nThreads);
+#endif
+    const R G = gridSize;
+    const R tMin = 0.001, tMax = 1e20, nudge = 1e-4;
+    const R rayArea = (G * G) / R(int64_t(nx) * int64_t(ny));
+    std::vector<R> kk(nFreqs);
+    for (int64_t f = 0; f < nFreqs; ++f) kk[f] = 2.0 * M_PI / (299792458.0 / freqHz[f]);
+    const size_t nc = (size_t)nFreqs * 2;
+    std::vector<double> rowRe((size_t)ny * nc), rowIm((size_t)ny * nc);
+    for (int64_t a = 0; a < nAngles; ++a) {
+        Frame<R> fr = make_frame<R>(thetaDeg[a], phiDeg[a], G);
+        const R th = thetaDeg[a] * M_PI / 180.0, ph = phiDeg[a] * M_PI / 180.0;
+        const V3<R> eRx[2] = {V3<R>(-std::sin(ph), std::cos(ph), 0.0),
+                              V3<R>(std::cos(th) * std::cos(ph), std::cos(th) * std::sin(ph), -std::sin(th))};
+        const R plane = dot(fr.dir, fr.llc);
+#pragma omp parallel for schedule(dynamic)
+        for (int32_t j = 0; j < ny; ++j) {
+            Counters cnt;
+            std::vector<double> accRe(nc, 0.0), accIm(nc, 0.0);
+            for (int32_t i = 0; i < nx; ++i) {
+                R u = (R(i) + 0.5) / R(nx);
+                R v = (R(j) + 0.5) / R(ny);
+                V3<R> o = fr.llc + scale(u, fr.u) + scale(v, fr.v);
+                V3<R> d = fr.rayDir;
+                V3<R> E[2] = {eRx[0], eRx[1]};   // field on the current segment
+                V3<R> Elast[2], nLast, dLast, pLast;
+                int32_t count = 0;
+                R dist = 0.0;
+                for (int32_t b = 0; b < maxBounces; ++b) {
+                    Hit<R> h;
+                    bool hit = accel == 1 ? walk_tree(tris, tb.nodes, o, d, tMin, tMax, h, cnt)
+                                          : walk_all(original, o, d, tMin, tMax, h, cnt);
+                    if (!hit) break;
+                    nLast = h.n;
+                    dLast = d;
+                    pLast = h.p;
+                    count++;
+                    dist += h.t;
+                    for (int p = 0; p < 2; ++p) {
+                        Elast[p] = E[p];
+                        E[p] = scale(2.0 * dot(h.n, E[p]), h.n) - E[p];
+                    }
+                    d = unit(d - scale(R(2.0) * dot(d, h.n), h.n));
+                    o = h.p + scale(nudge, h.n);
+                }
+                if (count == 0) continue;
+                R Rn = 1.0;
+                for (int32_t b = 0; b < count; ++b) Rn *= reflConst;
+                if (!(dot(nLast, -dLast) > 0.0)) continue;
+                const R path = dist + (plane - dot(fr.dir, pLast));
+                R amp[2];
+                for (int p = 0; p < 2; ++p) amp[p] = 2.0 * Rn * dot(eRx[p], cross(nLast, cross(dLast, Elast[p])));
+                for (int64_t f = 0; f < nFreqs; ++f) {
+                    const R k = kk[f];
+                    const R phase = std::fmod(k * path, 2.0 * M_PI);
+                    const R s = std::sin(phase), c = std::cos(phase);
+                    for (int p = 0; p < 2; ++p) {
+                        const R mag = (k * rayArea / (4.0 * M_PI)) * amp[p];
+                        accRe[2 * f + p] += -mag * s;
+                        accIm[2 * f + p] += mag * c;
+                    }
+                }
+            }
+            for (size_t c = 0; c < nc; ++c) {
+                rowRe[(size_t)j * nc + c] = accRe[c];
+                rowIm[(size_t)j * nc + c] = accIm[c];
+            }
+        }
+        for (size_t c = 0; c < nc; ++c) {
+            double re = 0, im = 0;
+            for (int32_t j = 0; j < ny; ++j) { re += rowRe[(size_t)j * nc + c]; im += rowIm[(size_t)j * nc + c]; }
+            outRe[(size_t)a * nc + c] = re;
+            outIm[(size_t)a * nc + c] = im;
+        }
+    }
+    return 0;
+}
+
 }  // namespace
 
 extern "C" {
+
+// Polarised FP64 sweep (see sweep_pol_impl); accel as oracle_sweep.
+int oracle_sweep_pol(const float* xyz, int64_t nverts, const uint32_t* idx, int64_t ntris, double modelScale,
+                     const double* thetaDeg, const double* phiDeg, int64_t nAngles, const double* freqHz,
+                     int64_t nFreqs, int32_t nx, int32_t ny, double gridSize, int32_t maxBounces, double reflConst,
+                     int32_t accel, int32_t nThreads, double* outRe, double* outIm) {
+    return sweep_pol_impl(xyz, nverts, idx, ntris, modelScale, thetaDeg, phiDeg, nAngles, freqHz, nFreqs, nx, ny,
+                          gridSize, maxBounces, reflConst, accel, nThreads, outRe, outIm);
+}
 
 // Full sweep: for every angle trace nx*ny rays (reference semantics) and reduce
 // the PO field for every frequency.  precision: 64 or 32.  accel: 1 = reference

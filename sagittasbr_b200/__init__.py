@@ -137,7 +137,7 @@ class JobSpec:
 
 @dataclass
 class SweepResult:
-    field: np.ndarray      # complex128 [n_samples] (job, angle, freq order)
+    field: np.ndarray      # complex128 [n_samples] (job, angle, freq order); [n_samples, 2] (HH, VV) polarised
     sigma_m2: np.ndarray
     rcs_dbsm: np.ndarray
     stats: np.ndarray      # uint64 [n_job_angles, 4]: rays, hit rays, bounces, queries
@@ -174,11 +174,11 @@ class Plan:
     """Prepared sweep (sbr_plan): frames, work items and result buffers on the GPU."""
 
     def __init__(self, scene: Scene, jobs: Sequence[JobSpec], mode=MODE_BATCHED, precision=PREC_MIXED,
-                 stream=None, use_graph=False, ctas_per_sm=0, first_hit=None):
+                 stream=None, use_graph=False, ctas_per_sm=0, first_hit=None, polarization=POL_SCALAR):
         self.scene = scene
         self.jobs = list(jobs)
         self._jc = _jobs_c(self.jobs)
-        o = _opts(mode, precision, stream=stream, use_graph=use_graph, ctas_per_sm=ctas_per_sm,
+        o = _opts(mode, precision, polarization, stream=stream, use_graph=use_graph, ctas_per_sm=ctas_per_sm,
                   first_hit=FIRST_HIT_TRAVERSE if first_hit is None else first_hit)
         h = C.c_void_p()
         check(lib().sbr_plan_create(scene.handle, self._jc, len(self.jobs), C.byref(o), C.byref(h)),
@@ -194,14 +194,15 @@ class Plan:
     def results(self) -> SweepResult:
         n = self.info["n_samples"]
         na = self.info["n_job_angles"]
-        f = np.zeros(2 * n)
-        s = np.zeros(n)
-        d = np.zeros(n)
+        npol = self.info["n_pol"]
+        f = np.zeros(2 * n * npol)
+        s = np.zeros(n * npol)
+        d = np.zeros(n * npol)
         st = np.zeros(4 * na, dtype=np.uint64)
         r = _lib.Result()
         r.field, r.sigma_m2, r.rcs_dbsm, r.stats = f.ctypes.data, s.ctypes.data, d.ctypes.data, st.ctypes.data
         check(lib().sbr_plan_results(self._h, C.byref(r)), "sbr_plan_results")
-        return SweepResult(f[0::2] + 1j * f[1::2], s, d, st.reshape(na, 4), r.device_ms)
+        return _result(f, s, d, st.reshape(na, 4), r.device_ms, npol)
 
     def device_results(self):
         pf, ps = C.c_void_p(), C.c_void_p()
@@ -220,23 +221,33 @@ class Plan:
             pass
 
 
+def _result(f, s, d, st, ms, npol):
+    field = f[0::2] + 1j * f[1::2]
+    if npol > 1:
+        field, s, d = field.reshape(-1, npol), s.reshape(-1, npol), d.reshape(-1, npol)
+    return SweepResult(field, s, d, st, ms)
+
+
 def run(scene: Scene, jobs: Sequence[JobSpec] | JobSpec, mode=MODE_BATCHED, precision=PREC_MIXED,
-        stream=None, first_hit=None) -> SweepResult:
-    """One call through sbr_run: host arrays in, host arrays out."""
+        stream=None, first_hit=None, polarization=POL_SCALAR) -> SweepResult:
+    """One call through sbr_run: host arrays in, host arrays out.  With
+    polarization=POL_HHVV the fields, sigma and dBsm carry a trailing (HH, VV) axis."""
     if isinstance(jobs, JobSpec):
         jobs = [jobs]
     jc = _jobs_c(jobs)
+    npol = 2 if polarization == POL_HHVV else 1
     n = sum(j.n_angles * j.n_freqs for j in jobs)
     na = sum(j.n_angles for j in jobs)
-    f = np.zeros(2 * n)
-    s = np.zeros(n)
-    d = np.zeros(n)
+    f = np.zeros(2 * n * npol)
+    s = np.zeros(n * npol)
+    d = np.zeros(n * npol)
     st = np.zeros(4 * na, dtype=np.uint64)
     r = _lib.Result()
     r.field, r.sigma_m2, r.rcs_dbsm, r.stats = f.ctypes.data, s.ctypes.data, d.ctypes.data, st.ctypes.data
-    o = _opts(mode, precision, stream=stream, first_hit=FIRST_HIT_TRAVERSE if first_hit is None else first_hit)
+    o = _opts(mode, precision, polarization, stream=stream,
+              first_hit=FIRST_HIT_TRAVERSE if first_hit is None else first_hit)
     check(lib().sbr_run(scene.handle, jc, len(jobs), C.byref(r), C.byref(o)), "sbr_run")
-    return SweepResult(f[0::2] + 1j * f[1::2], s, d, st.reshape(na, 4), r.device_ms)
+    return _result(f, s, d, st.reshape(na, 4), r.device_ms, npol)
 
 
 def trace_records(scene: Scene, job: JobSpec, precision=PREC_MIXED, first_hit=None) -> np.ndarray:

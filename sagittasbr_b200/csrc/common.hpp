@@ -89,6 +89,17 @@ struct __align__(16) Segment {
     double ps[4], pt[4];
     int64_t zbase;        // first first-hit buffer entry of this segment within its chunk
 };
+// Per (job, angle) data of SBR_POL_HHVV plans: the transmit / receive unit vectors
+// e_H = phi-hat = (-sin phi, cos phi, 0) and e_V = theta-hat =
+// (cos theta cos phi, cos theta sin phi, -sin theta), and the distance of the
+// reference launch plane (the reference's corner at 10 G) from the origin along the
+// incidence direction, which the exit path is measured back to.
+struct SegPol {
+    double eh[3], ev[3];
+    double plane;
+    double pad;
+};
+
 struct JobConst {
     int32_t nx, ny;
     int32_t n_freqs;
@@ -102,13 +113,15 @@ struct JobConst {
 };
 
 // Per frequency: k, the PO scale k*A/(4 pi) (ray area of the owning job), the
-// fixed-point quantum of the field accumulators, and FP32 copies used by the
+// fixed-point quantum of the field accumulators, the phase of a unit path length
+// of the scalar term in turns (2 k / (2 pi)), and FP32 copies used by the
 // reference FP32 arithmetic.
 struct FreqConst {
     double k;
     double scale;         // k * rayArea / (4 pi)
     double quantum;       // field value of one accumulator unit
     double inv_quantum;
+    double turns;         // k / pi
     float kf;
     float scalef;
 };

@@ -93,6 +93,7 @@ void release(sbr_plan* p) {
     cudaFree(p->d_stats);
     cudaFree(p->d_queue);
     cudaFree(p->d_zbuf);
+    cudaFree(p->d_segpol);
     if (p->ev0) cudaEventDestroy(p->ev0);
     if (p->ev1) cudaEventDestroy(p->ev1);
     delete p;
@@ -116,13 +117,19 @@ sbr_status validate_run(const sbr_scene* s, const sbr_job* jobs, size_t n_jobs, 
     if (!s || (!jobs && n_jobs)) return fail(SBR_ERR_INVALID_ARG, "null scene or jobs");
     if (o.mode != SBR_MODE_BATCHED && o.mode != SBR_MODE_PER_ANGLE) return fail(SBR_ERR_INVALID_ARG, "bad mode");
     if (o.precision < SBR_PREC_MIXED || o.precision > SBR_PREC_FP64) return fail(SBR_ERR_INVALID_ARG, "bad precision");
-    if (o.polarization != SBR_POL_SCALAR) return fail(SBR_ERR_UNSUPPORTED, "polarisation tracking is not built");
+    if (o.polarization != SBR_POL_SCALAR && o.polarization != SBR_POL_HHVV)
+        return fail(SBR_ERR_INVALID_ARG, "bad polarization");
+    const bool pol = o.polarization == SBR_POL_HHVV;
+    if (pol && o.precision == SBR_PREC_FP32)
+        return fail(SBR_ERR_UNSUPPORTED, "polarisation tracking runs in SBR_PREC_MIXED or SBR_PREC_FP64");
     for (size_t j = 0; j < n_jobs; ++j) {
         const sbr_job& J = jobs[j];
         if (J.n_angles < 0 || (J.n_angles > 0 && (!J.theta_deg || !J.phi_deg)))
             return fail(SBR_ERR_INVALID_ARG, "job angles");
         if (J.n_freqs < 1 || !J.freq_hz) return fail(SBR_ERR_INVALID_ARG, "job needs at least one frequency");
         if (J.n_freqs > max_freqs_per_job()) return fail(SBR_ERR_TOO_LARGE, "more than 128 frequencies in one job");
+        if (pol && 2 * J.n_freqs > max_freqs_per_job())
+            return fail(SBR_ERR_TOO_LARGE, "more than 64 frequencies in one polarised job");
         if (J.nx <= 0 || J.ny <= 0) return fail(SBR_ERR_INVALID_ARG, "n_x and n_y must be positive");
         if ((int64_t)J.nx * (int64_t)J.ny > (int64_t(1) << 31) - 1)
             return fail(SBR_ERR_TOO_LARGE, "more than 2^31-1 rays per angle");
@@ -174,6 +181,7 @@ sbr_status build_tables(const sbr_scene* s, const sbr_job* jobs, size_t n_jobs, 
             double lambda = c0 / J.freq_hz[f];
             fc.k = 2.0 * M_PI / lambda;
             fc.scale = fc.k * area / (4.0 * M_PI);
+            fc.turns = fc.k / M_PI;
             float lambdaf = 299792458.0f / float(J.freq_hz[f]);
             fc.kf = 2.0f * float(M_PI) / lambdaf;
             fc.scalef = fc.kf * areaf / (4.0f * float(M_PI));
@@ -335,6 +343,25 @@ sbr_status sbr_plan_create(sbr_scene* s, const sbr_job* jobs, size_t n_jobs, con
     p->n_samples = tot.n_samples;
     p->n_rays_clipped = tot.n_rays_clipped;
     p->n_rays_grid = tot.n_rays_grid;
+    p->n_pol = p->pol == SBR_POL_HHVV ? 2 : 1;
+    if (p->n_pol == 2) {
+        // per angle: HH / VV unit vectors and the reference launch plane; the
+        // accumulator units are per (sample, polarisation)
+        p->segpol.resize(p->segs.size());
+        for (size_t g = 0; g < p->segs.size(); ++g) {
+            const Segment& G = p->segs[g];
+            const double th = jobs[G.job].theta_deg[G.angle] * M_PI / 180.0;
+            const double ph = jobs[G.job].phi_deg[G.angle] * M_PI / 180.0;
+            SegPol& q = p->segpol[g];
+            q.eh[0] = -std::sin(ph); q.eh[1] = std::cos(ph); q.eh[2] = 0.0;
+            q.ev[0] = std::cos(th) * std::cos(ph); q.ev[1] = std::cos(th) * std::sin(ph); q.ev[2] = -std::sin(th);
+            q.plane = G.dir[0] * G.llc[0] + G.dir[1] * G.llc[1] + G.dir[2] * G.llc[2] + G.shift;
+            q.pad = 0.0;
+        }
+        std::vector<double> qp(2 * p->quantum.size());
+        for (size_t s = 0; s < p->quantum.size(); ++s) qp[2 * s] = qp[2 * s + 1] = p->quantum[s];
+        p->quantum.swap(qp);
+    }
 
     // first-hit rasterisation (batched FP32 / mixed): chunks of consecutive
     // segments whose per-pixel first-hit buffers fit a fixed budget
@@ -377,9 +404,10 @@ sbr_status sbr_plan_create(sbr_scene* s, const sbr_job* jobs, size_t n_jobs, con
     if ((st = upload(&p->d_segs, p->segs, b)) != SBR_OK || (st = upload(&p->d_seg_base, p->seg_base, b)) != SBR_OK ||
         (st = upload(&p->d_jobs, p->jobs, b)) != SBR_OK || (st = upload(&p->d_freqs, p->freqs, b)) != SBR_OK ||
         (st = upload(&p->d_quantum, p->quantum, b)) != SBR_OK ||
-        (st = zalloc(&p->d_acc, 2 * (size_t)p->n_samples * kAccReplicas, b)) != SBR_OK ||
+        (p->n_pol == 2 && (st = upload(&p->d_segpol, p->segpol, b)) != SBR_OK) ||
+        (st = zalloc(&p->d_acc, 2 * (size_t)p->n_samples * p->n_pol * kAccReplicas, b)) != SBR_OK ||
         (st = zalloc(&p->d_acc_stats, 4 * (size_t)p->n_segs, b)) != SBR_OK ||
-        (st = zalloc(&p->d_field, 2 * (size_t)p->n_samples, b)) != SBR_OK ||
+        (st = zalloc(&p->d_field, 2 * (size_t)p->n_samples * p->n_pol, b)) != SBR_OK ||
         (st = zalloc(&p->d_stats, 4 * (size_t)p->n_segs, b)) != SBR_OK ||
         (st = zalloc(&p->d_queue, 1 + (size_t)p->n_samples + p->chunks.size(), b)) != SBR_OK) {
         release(p);
@@ -431,14 +459,15 @@ sbr_status sbr_plan_results(sbr_plan* p, sbr_result* out) {
     float ms = 0.0f;
     SBR_CUDA(cudaEventElapsedTime(&ms, p->ev0, p->ev1));
     out->device_ms = ms;
-    std::vector<double> f(2 * (size_t)p->n_samples);
-    if (p->n_samples)
+    const int64_t n_out = p->n_samples * p->n_pol;
+    std::vector<double> f(2 * (size_t)n_out);
+    if (n_out)
         SBR_CUDA(cudaMemcpyAsync(f.data(), p->d_field, f.size() * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
     if (out->stats && p->n_segs)
         SBR_CUDA(cudaMemcpyAsync(out->stats, p->d_stats, 4 * (size_t)p->n_segs * sizeof(uint64_t),
                                  cudaMemcpyDeviceToHost, p->stream));
     SBR_CUDA(cudaStreamSynchronize(p->stream));
-    for (int64_t i = 0; i < p->n_samples; ++i) {
+    for (int64_t i = 0; i < n_out; ++i) {
         double re = f[2 * i], im = f[2 * i + 1];
         if (out->field) { out->field[2 * i] = re; out->field[2 * i + 1] = im; }
         double sigma = 4.0 * M_PI * (re * re + im * im);
@@ -462,7 +491,7 @@ sbr_status sbr_plan_info_get(const sbr_plan* p, sbr_plan_info* out) {
     out->n_items = p->n_items;
     out->n_rays_clipped = p->n_rays_clipped;
     out->n_rays_grid = p->n_rays_grid;
-    out->n_pol = 1;
+    out->n_pol = p->n_pol;
     int64_t launches = 1;
     if (p->mode == SBR_MODE_BATCHED && p->raster) {
         for (const auto& ch : p->chunks) launches += 1 + (ch.item_end > ch.item_begin ? 1 : 0);
@@ -476,8 +505,9 @@ sbr_status sbr_plan_info_get(const sbr_plan* p, sbr_plan_info* out) {
     out->device_bytes = p->device_bytes;
     out->h2d_bytes = (int64_t)(p->segs.size() * sizeof(Segment) + p->seg_base.size() * sizeof(int64_t) +
                                p->jobs.size() * sizeof(JobConst) + p->freqs.size() * sizeof(FreqConst) +
-                               p->quantum.size() * sizeof(double));
-    out->d2h_bytes = (int64_t)(2 * p->n_samples * sizeof(double) + 4 * p->n_segs * sizeof(uint64_t) + sizeof(uint32_t));
+                               p->quantum.size() * sizeof(double) + p->segpol.size() * sizeof(SegPol));
+    out->d2h_bytes = (int64_t)(2 * p->n_samples * p->n_pol * sizeof(double) + 4 * p->n_segs * sizeof(uint64_t) +
+                               sizeof(uint32_t));
     return SBR_OK;
 }
 
@@ -500,8 +530,12 @@ sbr_status sbr_run(sbr_scene* s, const sbr_job* jobs, size_t n_jobs, sbr_result*
 
 sbr_status sbr_trace_records(sbr_scene* s, const sbr_job* job, const sbr_run_opts* opts, sbr_ray_record* out) {
     if (!s || !job || !out) return fail(SBR_ERR_INVALID_ARG, "null argument");
+    // hit records do not depend on the polarisation: trace them with the scalar plan
+    sbr_run_opts o{};
+    if (opts) o = *opts;
+    o.polarization = SBR_POL_SCALAR;
     sbr_plan* p = nullptr;
-    sbr_status st = sbr_plan_create(s, job, 1, opts, &p);
+    sbr_status st = sbr_plan_create(s, job, 1, &o, &p);
     if (st != SBR_OK) return st;
     long long n = (long long)job->n_angles * job->nx * job->ny;
     sbr_ray_record* d = nullptr;

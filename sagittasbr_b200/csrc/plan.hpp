@@ -52,7 +52,9 @@ struct sbr_plan {
     std::vector<int64_t> seg_base;     // [n_segs + 1] first item of each segment
     std::vector<sbr::JobConst> jobs;
     std::vector<sbr::FreqConst> freqs;
-    std::vector<double> quantum;       // per sample
+    std::vector<double> quantum;       // per sample and polarisation
+    std::vector<sbr::SegPol> segpol;   // per segment (SBR_POL_HHVV)
+    int n_pol = 1;
     int64_t n_segs = 0, n_items = 0, n_samples = 0;
     int64_t n_rays_clipped = 0, n_rays_grid = 0;
     int k_max = 1;
@@ -65,6 +67,7 @@ struct sbr_plan {
     sbr::JobConst* d_jobs = nullptr;
     sbr::FreqConst* d_freqs = nullptr;
     double* d_quantum = nullptr;
+    sbr::SegPol* d_segpol = nullptr;
     unsigned long long* d_acc = nullptr;
     unsigned long long* d_acc_stats = nullptr;
     double* d_field = nullptr;

@@ -37,7 +37,8 @@ struct TraceParams {
     const FreqConst* freqs;
     int64_t item_begin, item_end;  // items handled by this launch
     unsigned long long* queue;     // work-queue head of this launch
-    unsigned long long* acc;       // [n_samples][n_rep][2] fixed-point field accumulators
+    const SegPol* segpol;          // [n_segs], SBR_POL_HHVV plans only
+    unsigned long long* acc;       // [n_samples][n_pol][n_rep][2] fixed-point field accumulators
     unsigned long long* acc_stats; // [n_segs * 4]
     uint32_t* err;
     const volatile int32_t* cancel;
@@ -45,8 +46,25 @@ struct TraceParams {
     unsigned long long* zbuf;      // first-hit buffer of the launch's chunk, or null (walk the BVH)
 };
 
-constexpr int kMaxK = 128;   // frequencies per job
-constexpr int kRegK = 4;     // per-lane accumulation up to this many frequencies
+constexpr int kMaxK = 128;   // accumulation channels (frequencies x polarisations) per job
+constexpr int kRegK = 4;     // per-lane accumulation up to this many channels
+
+// Accumulator layouts of the PO epilogue.  A job's channels are its frequencies
+// (scalar plans) or its (frequency, polarisation) pairs, channel 2k + p (HHVV plans).
+//   EPI_LANE1, EPI_LANE4: every lane sums the terms of its own rays for up to 1 / 4
+//                         channels (registers sized to the plan's channel count)
+//   EPI_T64, EPI_T128:    lanes own channels lane, lane + 32, ...; each finished ray
+//                         is broadcast to the warp (up to 64 / 128 channels)
+enum : int { EPI_LANE1 = 0, EPI_LANE4 = 1, EPI_T64 = 2, EPI_T128 = 3 };
+template <int EPI>
+struct Epi {
+    static constexpr bool kTransposed = EPI >= EPI_T64;
+    static constexpr int kAcc = EPI == EPI_LANE1 ? 1 : EPI == EPI_LANE4 ? 4 : EPI == EPI_T64 ? 2 : 4;
+    static constexpr int kChannels = kTransposed ? 32 * kAcc : kAcc;
+};
+inline int pick_epi(int channels) {
+    return channels <= 1 ? EPI_LANE1 : channels <= kRegK ? EPI_LANE4 : channels <= 64 ? EPI_T64 : EPI_T128;
+}
 // Resident CTAs (of 4 warps) per SM the kernels are register-budgeted for:
 // 6 -> at most 85 registers per thread, 24 warps per SM.
 constexpr int kMinCtasPerSm = 6;
@@ -72,7 +90,38 @@ struct RayOut {
     double L;
     float cosT, Rn;
     double cosD, RnD;
+    double pa[2];  // SBR_POL_HHVV: co-polarised amplitudes (HH, VV)
+    double Lp;     // SBR_POL_HHVV: path launch plane -> exit point -> launch plane
 };
+
+// Polarisation state of SBR_POL_HHVV plans: the HH and VV incident fields as they
+// arrive at the ray's latest hit (unit vectors; PEC reflection keeps them real).
+struct PolF {
+    F3 h, v;
+};
+struct PolD {
+    D3 h, v;
+};
+
+// PEC boundary condition: the reflected field is 2 (n.E) n - E (tangential part
+// reversed, normal part kept).
+__device__ __forceinline__ F3 pec_reflect(F3 e, F3 n) {
+    const float s = 2.0f * dot(n, e);
+    return f3(s * n.x - e.x, s * n.y - e.y, s * n.z - e.z);
+}
+__device__ __forceinline__ D3 pec_reflect(D3 e, D3 n) {
+    const double s = 2.0 * dot(n, e);
+    return D3{s * n.x - e.x, s * n.y - e.y, s * n.z - e.z};
+}
+
+// Co-polarised exit amplitude: 2 R^n e.(n x (d_in x E_in)), the direction of the PO
+// surface current n x H_in on the last surface projected on the receive
+// polarisation e, with the scalar term's ray-tube weighting.  For a single bounce
+// (E_in = e, d_in = -s) it equals the scalar amplitude 2 cos(theta) R^n.
+template <class V, class R>
+__device__ __forceinline__ R pol_amp(V e, V n, V d, V E, R twoRn) {
+    return twoRn * dot(e, cross(n, cross(d, E)));
+}
 
 // ------------------------------------------------------------ FP32 / mixed
 // Origin of the primary ray of pixel (i, j) (src/cuda/rtKernels.cu:120-123); the
@@ -107,9 +156,9 @@ __device__ __forceinline__ void start_f(RayF& r, const Segment& G, const JobCons
 // One closest-hit query, then reflect and nudge; true when the ray is finished.
 // The first query is read from the first-hit buffer when there is one (and the
 // entry is restored to empty for the next chunk).
-template <int PREC, bool REC>
-__device__ __forceinline__ bool step_f(RayF& r, const SceneView& S, int maxB, uint32_t& err, sbr_ray_record* rec,
-                                       unsigned long long* zbuf) {
+template <int PREC, bool REC, bool POL>
+__device__ __forceinline__ bool step_f(RayF& r, PolF& e, const SceneView& S, int maxB, uint32_t& err,
+                                       sbr_ray_record* rec, unsigned long long* zbuf) {
     float tB = 1e20f;
     int slot;
     if (zbuf != nullptr && r.count == 0) {
@@ -124,6 +173,12 @@ __device__ __forceinline__ bool step_f(RayF& r, const SceneView& S, int maxB, ui
     if (slot < 0) return true;
     const GTri* T = S.tris + slot;
     const F3 n = f3(__ldg(&T->p.w), __ldg(&T->e1.w), __ldg(&T->e2.w));
+    if constexpr (POL) {
+        if (r.count > 0) {  // the field left the previous hit reflected there
+            e.h = pec_reflect(e.h, r.nl);
+            e.v = pec_reflect(e.v, r.nl);
+        }
+    }
     r.nl = n;
     r.dl = r.d;
     ++r.count;
@@ -166,13 +221,20 @@ __device__ __forceinline__ void start_d(RayD& r, const Segment& G, const JobCons
     r.count = 0;
 }
 
-template <bool REC>
-__device__ __forceinline__ bool step_d(RayD& r, const SceneView& S, int maxB, uint32_t& err, sbr_ray_record* rec) {
+template <bool REC, bool POL>
+__device__ __forceinline__ bool step_d(RayD& r, PolD& e, const SceneView& S, int maxB, uint32_t& err,
+                                       sbr_ray_record* rec) {
     double tB = 1e20;
     const int slot = Walker<true>::closest(S, r.o, r.d, 1.0e-3, tB, err);
     if (slot < 0) return true;
     const GTri64& T = S.tris64[slot];
     const D3 n{T.n[0], T.n[1], T.n[2]};
+    if constexpr (POL) {
+        if (r.count > 0) {
+            e.h = pec_reflect(e.h, r.nl);
+            e.v = pec_reflect(e.v, r.nl);
+        }
+    }
     r.nl = n;
     r.dl = r.d;
     ++r.count;
@@ -200,10 +262,20 @@ __device__ __forceinline__ RayOut finish_d(const RayD& r, const JobConst& J) {
     return o;
 }
 
+// sin and cos of 2 pi x for a phase x given in turns (FP64): the whole turns are
+// removed exactly (x - rint(x) is exact for |x| < 2^52), the remainder in
+// [-1/2, 1/2] is rounded to FP32 (an absolute error below 3e-8 turns) and its
+// sine and cosine are taken in FP32.
+__device__ __forceinline__ void sincos_turns(double x, float& s, float& c) {
+    const float r = float(x - rint(x));
+    __sincosf(6.28318530717958647692f * r, &s, &c);
+}
+
 // PO term of one ray at one frequency, added to (re, im).
 //  FP32: the reference FP32 arithmetic (phase fmodf in FP32).
-//  MIXED: phase 2 k L reduced in FP64 by two-constant Cody-Waite, sin/cos of the
-//         reduced FP32 angle, magnitude in FP64.
+//  MIXED: phase 2 k L = 2 pi (k / pi) L reduced in turns (sincos_turns); the
+//         term is summed without the factor k A / (4 pi), which the item fold
+//         applies once per channel.
 //  FP64: the reference USE_DOUBLE arithmetic.
 __device__ __forceinline__ void po_term(int prec, const FreqConst& F, const RayOut& r, double& re, double& im) {
     if (prec == SBR_PREC_FP32) {
@@ -216,18 +288,11 @@ __device__ __forceinline__ void po_term(int prec, const FreqConst& F, const RayO
         re += double(-mag * s);
         im += double(mag * c);
     } else if (prec == SBR_PREC_MIXED) {
-        const double twoPiHi = 6.283185307179586232;      // nearest double to 2 pi
-        const double twoPiLo = 2.4492935982947064e-16;     // 2 pi - twoPiHi
-        const double invTwoPi = 0.15915494309189534561;
-        const double ph = 2.0 * F.k * r.L;
-        const double q = rint(ph * invTwoPi);
-        double red = fma(-q, twoPiHi, ph);
-        red = fma(-q, twoPiLo, red);
         float s, c;
-        __sincosf(float(red), &s, &c);
-        const double mag = F.scale * double(r.amp);
-        re -= mag * double(s);
-        im += mag * double(c);
+        sincos_turns(F.turns * r.L, s, c);
+        const double a = double(r.amp);
+        re -= a * double(s);
+        im += a * double(c);
     } else {
         const double twoPi = 2.0 * 3.14159265358979323846;
         const double phase = fmod((2.0 * F.k) * r.L, twoPi);
@@ -235,6 +300,59 @@ __device__ __forceinline__ void po_term(int prec, const FreqConst& F, const RayO
         double s, c;
         sincos(phase, &s, &c);
         re += -mag * s;
+        im += mag * c;
+    }
+}
+
+// Polarised exit terms of a finished ray (SBR_POL_HHVV): the HH and VV amplitudes
+// and the physical exit path L + (plane - s.p_last), i.e. the path from the launch
+// plane to the last hit point and back to the plane (the scalar term uses 2 L).
+// The last hit point is the ray origin minus its 1e-4 nudge.  Rays the scalar
+// gate drops (no hit, or cos(theta) <= 0) add nothing here either.
+__device__ __forceinline__ void pol_finish_f(RayOut& o, const RayF& r, const PolF& e, const SegPol& P,
+                                             const Segment& G) {
+    o.pa[0] = 0.0;
+    o.pa[1] = 0.0;
+    o.Lp = 0.0;
+    if (o.amp == 0.0f) return;
+    const float twoRn = 2.0f * o.Rn;
+    const F3 eh = f3(float(P.eh[0]), float(P.eh[1]), float(P.eh[2]));
+    const F3 ev = f3(float(P.ev[0]), float(P.ev[1]), float(P.ev[2]));
+    o.pa[0] = double(pol_amp(eh, r.nl, r.dl, e.h, twoRn));
+    o.pa[1] = double(pol_amp(ev, r.nl, r.dl, e.v, twoRn));
+    const F3 p = r.o - 1.0e-4f * r.nl;
+    o.Lp = r.L + P.plane - (G.dir[0] * double(p.x) + G.dir[1] * double(p.y) + G.dir[2] * double(p.z));
+}
+__device__ __forceinline__ void pol_finish_d(RayOut& o, const RayD& r, const PolD& e, const SegPol& P,
+                                             const Segment& G) {
+    o.pa[0] = 0.0;
+    o.pa[1] = 0.0;
+    o.Lp = 0.0;
+    if (o.amp == 0.0f) return;
+    const double twoRn = 2.0 * o.RnD;
+    o.pa[0] = pol_amp(D3{P.eh[0], P.eh[1], P.eh[2]}, r.nl, r.dl, e.h, twoRn);
+    o.pa[1] = pol_amp(D3{P.ev[0], P.ev[1], P.ev[2]}, r.nl, r.dl, e.v, twoRn);
+    const D3 p = r.o - 1.0e-4 * r.nl;
+    o.Lp = r.L + P.plane - dot(D3{G.dir[0], G.dir[1], G.dir[2]}, p);
+}
+
+// Polarised PO term of one ray at one frequency: phase k Lp, magnitude
+// k A / (4 pi) * amplitude, added as (-mag sin, mag cos) like the scalar term.
+//  MIXED: k Lp = 2 pi (k / (2 pi)) Lp reduced in turns (sincos_turns), summed
+//         without the factor k A / (4 pi) like the scalar MIXED term.
+//  FP64:  fmod and sincos in FP64.
+__device__ __forceinline__ void po_term_pol(int prec, const FreqConst& F, double Lp, double amp, double& re,
+                                            double& im) {
+    if (prec == SBR_PREC_MIXED) {
+        float s, c;
+        sincos_turns(F.turns * (0.5 * Lp), s, c);
+        re -= amp * double(s);
+        im += amp * double(c);
+    } else {
+        double s, c;
+        sincos(fmod(F.k * Lp, 2.0 * 3.14159265358979323846), &s, &c);
+        const double mag = F.scale * amp;
+        re -= mag * s;
         im += mag * c;
     }
 }
@@ -249,6 +367,12 @@ __device__ __forceinline__ int find_segment(const int64_t* base, int n, int64_t 
     return lo;
 }
 
+// Accumulator units per unit of a lane sum: MIXED sums leave out k A / (4 pi).
+template <int PREC>
+__device__ __forceinline__ double fold_factor(const FreqConst& F) {
+    return PREC == SBR_PREC_MIXED ? F.scale * F.inv_quantum : F.inv_quantum;
+}
+
 __device__ __forceinline__ void add_fixed(unsigned long long* acc, double v, double invQ) {
     const long long q = __double2ll_rn(v * invQ);
     if (q != 0) atomicAdd(acc, (unsigned long long)q);
@@ -261,11 +385,13 @@ __device__ __forceinline__ void add_fixed(unsigned long long* acc, double v, dou
 // the warp reduces them in a fixed order and adds the total, as int64 fixed
 // point, to one of the segment's accumulator replicas.  Which lane takes which
 // ray depends only on the item, so every sum is reproducible bit for bit.
-template <int PREC, bool TRANSPOSED, bool REC>
+template <int PREC, int EPI, bool REC, bool POL>
 __global__ void __launch_bounds__(kCtaThreads, kMinCtasPerSm) k_trace(const TraceParams P) {
     constexpr unsigned FULL = 0xffffffffu;
     constexpr bool F64 = PREC == SBR_PREC_FP64;
-    constexpr int NACC = TRANSPOSED ? kMaxK / 32 : kRegK;
+    constexpr bool TRANSPOSED = Epi<EPI>::kTransposed;
+    constexpr int NACC = Epi<EPI>::kAcc;
+    constexpr int NPOL = POL ? 2 : 1;
     const int lane = threadIdx.x & 31;
     const int warp_global = (int)((blockIdx.x * (unsigned)kCtaThreads + threadIdx.x) >> 5);
     const int rep = warp_global % P.n_rep;
@@ -293,6 +419,7 @@ __global__ void __launch_bounds__(kCtaThreads, kMinCtasPerSm) k_trace(const Trac
         const int b0 = int(item - G.item_base) * G.blocks_per_item;
         const int nslots = min(G.blocks_per_item, G.blocks - b0) * 32;
         const int i_end = G.i0 + G.ni, j_end = G.j0 + G.nj;
+        const int KC = K * NPOL;  // channels of this item
 
         double accRe[NACC], accIm[NACC];
 #pragma unroll
@@ -301,6 +428,9 @@ __global__ void __launch_bounds__(kCtaThreads, kMinCtasPerSm) k_trace(const Trac
 
         RayF rf;
         RayD rd;
+        PolF ef;
+        PolD ed;
+        const SegPol* GP = POL ? P.segpol + seg : nullptr;
         bool active = false;
         int queries = 0;
         sbr_ray_record* rec = nullptr;
@@ -318,6 +448,15 @@ __global__ void __launch_bounds__(kCtaThreads, kMinCtasPerSm) k_trace(const Trac
                     if (i < i_end && j < j_end) {
                         if (F64) start_d(rd, G, J, i, j);
                         else start_f<PREC>(rf, G, J, i, j);
+                        if constexpr (POL) {
+                            if (F64) {
+                                ed.h = D3{GP->eh[0], GP->eh[1], GP->eh[2]};
+                                ed.v = D3{GP->ev[0], GP->ev[1], GP->ev[2]};
+                            } else {
+                                ef.h = f3(float(GP->eh[0]), float(GP->eh[1]), float(GP->eh[2]));
+                                ef.v = f3(float(GP->ev[0]), float(GP->ev[1]), float(GP->ev[2]));
+                            }
+                        }
                         active = true;
                         queries = 0;
                         ++cRays;
@@ -334,12 +473,16 @@ __global__ void __launch_bounds__(kCtaThreads, kMinCtasPerSm) k_trace(const Trac
             RayOut out;
             out.amp = 0.0f;
             if (active) {
-                done = F64 ? step_d<REC>(rd, P.S, J.max_bounces, err, rec)
-                           : step_f<PREC, REC>(rf, P.S, J.max_bounces, err, rec, P.zbuf);
+                done = F64 ? step_d<REC, POL>(rd, ed, P.S, J.max_bounces, err, rec)
+                           : step_f<PREC, REC, POL>(rf, ef, P.S, J.max_bounces, err, rec, P.zbuf);
                 ++queries;
                 if (done) {
                     const int cnt = F64 ? rd.count : rf.count;
                     out = F64 ? finish_d(rd, J) : finish_f<PREC>(rf, J);
+                    if constexpr (POL) {
+                        if (F64) pol_finish_d(out, rd, ed, *GP, G);
+                        else pol_finish_f(out, rf, ef, *GP, G);
+                    }
                     cHit += cnt > 0;
                     cBounce += cnt;
                     cQuery += queries;
@@ -361,28 +504,41 @@ __global__ void __launch_bounds__(kCtaThreads, kMinCtasPerSm) k_trace(const Trac
             if (!TRANSPOSED) {
                 if (done && out.amp != 0.0f) {
 #pragma unroll
-                    for (int k = 0; k < kRegK; ++k)
-                        if (k < K) po_term(PREC, F[k], out, accRe[k], accIm[k]);
+                    for (int ch = 0; ch < NACC; ++ch) {
+                        if (ch < KC) {
+                            if constexpr (POL) po_term_pol(PREC, F[ch >> 1], out.Lp, out.pa[ch & 1], accRe[ch], accIm[ch]);
+                            else po_term(PREC, F[ch], out, accRe[ch], accIm[ch]);
+                        }
+                    }
                 }
             } else {
-                // lanes own frequencies lane, lane + 32, ...; finished rays are taken
-                // in lane order, so every frequency's sum has a fixed order
+                // lanes own channels lane, lane + 32, ...; finished rays are taken
+                // in lane order, so every channel's sum has a fixed order
                 unsigned m = __ballot_sync(FULL, done && out.amp != 0.0f);
                 while (m) {
                     const int src = __ffs(m) - 1;
                     m &= m - 1;
                     RayOut q;
-                    q.amp = __shfl_sync(FULL, out.amp, src);
-                    q.L = __shfl_sync(FULL, out.L, src);
-                    q.dist32 = __shfl_sync(FULL, out.dist32, src);
-                    q.cosT = __shfl_sync(FULL, out.cosT, src);
-                    q.Rn = __shfl_sync(FULL, out.Rn, src);
-                    q.cosD = F64 ? __shfl_sync(FULL, out.cosD, src) : 0.0;
-                    q.RnD = F64 ? __shfl_sync(FULL, out.RnD, src) : 0.0;
+                    if constexpr (POL) {
+                        q.pa[0] = __shfl_sync(FULL, out.pa[0], src);
+                        q.pa[1] = __shfl_sync(FULL, out.pa[1], src);
+                        q.Lp = __shfl_sync(FULL, out.Lp, src);
+                    } else {
+                        q.amp = __shfl_sync(FULL, out.amp, src);
+                        q.L = __shfl_sync(FULL, out.L, src);
+                        q.dist32 = __shfl_sync(FULL, out.dist32, src);
+                        q.cosT = __shfl_sync(FULL, out.cosT, src);
+                        q.Rn = __shfl_sync(FULL, out.Rn, src);
+                        q.cosD = F64 ? __shfl_sync(FULL, out.cosD, src) : 0.0;
+                        q.RnD = F64 ? __shfl_sync(FULL, out.RnD, src) : 0.0;
+                    }
 #pragma unroll
                     for (int c = 0; c < NACC; ++c) {
-                        const int k = c * 32 + lane;
-                        if (k < K) po_term(PREC, F[k], q, accRe[c], accIm[c]);
+                        const int ch = c * 32 + lane;
+                        if (ch < KC) {
+                            if constexpr (POL) po_term_pol(PREC, F[ch >> 1], q.Lp, q.pa[ch & 1], accRe[c], accIm[c]);
+                            else po_term(PREC, F[ch], q, accRe[c], accIm[c]);
+                        }
                     }
                 }
             }
@@ -393,33 +549,36 @@ __global__ void __launch_bounds__(kCtaThreads, kMinCtasPerSm) k_trace(const Trac
             if (!__any_sync(FULL, active)) refill();
         }
 
-        // ---- fold the item: lanes -> warp in a fixed order, then fixed point
-        const long long sbase = G.sample_base + kb;
+        // ---- fold the item: lanes -> warp in a fixed order, then fixed point.
+        // Channel ch of sample (sbase + k) lives at accumulator (sbase * NPOL + ch).
+        const long long cbase = (G.sample_base + kb) * NPOL;
         if (!TRANSPOSED) {
 #pragma unroll
-            for (int k = 0; k < kRegK; ++k) {
-                if (k < K) {
-                    double a = accRe[k], b = accIm[k];
+            for (int ch = 0; ch < NACC; ++ch) {
+                if (ch < KC) {
+                    double a = accRe[ch], b = accIm[ch];
 #pragma unroll
                     for (int off = 16; off > 0; off >>= 1) {
                         a += __shfl_xor_sync(FULL, a, off);
                         b += __shfl_xor_sync(FULL, b, off);
                     }
-                    if (lane == k) {
-                        unsigned long long* A = P.acc + 2 * ((sbase + k) * P.n_rep + rep);
-                        add_fixed(A, a, F[k].inv_quantum);
-                        add_fixed(A + 1, b, F[k].inv_quantum);
+                    if (lane == ch) {
+                        const double invQ = fold_factor<PREC>(F[POL ? ch >> 1 : ch]);
+                        unsigned long long* A = P.acc + 2 * ((cbase + ch) * P.n_rep + rep);
+                        add_fixed(A, a, invQ);
+                        add_fixed(A + 1, b, invQ);
                     }
                 }
             }
         } else {
 #pragma unroll
             for (int c = 0; c < NACC; ++c) {
-                const int k = c * 32 + lane;
-                if (k < K) {
-                    unsigned long long* A = P.acc + 2 * ((sbase + k) * P.n_rep + rep);
-                    add_fixed(A, accRe[c], F[k].inv_quantum);
-                    add_fixed(A + 1, accIm[c], F[k].inv_quantum);
+                const int ch = c * 32 + lane;
+                if (ch < KC) {
+                    const double invQ = fold_factor<PREC>(F[POL ? ch >> 1 : ch]);
+                    unsigned long long* A = P.acc + 2 * ((cbase + ch) * P.n_rep + rep);
+                    add_fixed(A, accRe[c], invQ);
+                    add_fixed(A + 1, accIm[c], invQ);
                 }
             }
         }
@@ -564,22 +723,41 @@ __global__ void k_fill_records(sbr_ray_record* r, long long n) {
 // --------------------------------------------------------------------- host
 namespace {
 
-template <int PREC, bool TR, bool REC>
+template <int PREC, int EPI, bool REC, bool POL>
 const void* kernel_ptr() {
-    return reinterpret_cast<const void*>(&k_trace<PREC, TR, REC>);
+    return reinterpret_cast<const void*>(&k_trace<PREC, EPI, REC, POL>);
 }
 
-const void* pick_kernel(int prec, bool transposed, bool rec) {
+template <int PREC, bool REC, bool POL>
+const void* pick_epi_kernel(int epi) {
+    switch (epi) {
+        case EPI_LANE1: return kernel_ptr<PREC, EPI_LANE1, REC, POL>();
+        case EPI_LANE4: return kernel_ptr<PREC, EPI_LANE4, REC, POL>();
+        case EPI_T64: return kernel_ptr<PREC, EPI_T64, REC, POL>();
+        default: return kernel_ptr<PREC, EPI_T128, REC, POL>();
+    }
+}
+
+// Trace kernel for a plan: precision, accumulator layout for `channels` (the
+// largest frequencies x polarisations of a launch), records, polarisation.
+// Record kernels come with the two general layouts only; polarised kernels in
+// MIXED and FP64 precision only (the host rejects the other combinations).
+const void* pick_kernel(int prec, int channels, bool rec, bool pol) {
+    int epi = pick_epi(channels);
+    if (rec) {
+        epi = epi <= EPI_LANE4 ? EPI_LANE4 : EPI_T128;
+        switch (prec) {
+            case SBR_PREC_MIXED: return pick_epi_kernel<SBR_PREC_MIXED, true, false>(epi);
+            case SBR_PREC_FP32: return pick_epi_kernel<SBR_PREC_FP32, true, false>(epi);
+            default: return pick_epi_kernel<SBR_PREC_FP64, true, false>(epi);
+        }
+    }
+    if (pol) return prec == SBR_PREC_FP64 ? pick_epi_kernel<SBR_PREC_FP64, false, true>(epi)
+                                          : pick_epi_kernel<SBR_PREC_MIXED, false, true>(epi);
     switch (prec) {
-        case SBR_PREC_MIXED:
-            if (rec) return transposed ? kernel_ptr<SBR_PREC_MIXED, true, true>() : kernel_ptr<SBR_PREC_MIXED, false, true>();
-            return transposed ? kernel_ptr<SBR_PREC_MIXED, true, false>() : kernel_ptr<SBR_PREC_MIXED, false, false>();
-        case SBR_PREC_FP32:
-            if (rec) return transposed ? kernel_ptr<SBR_PREC_FP32, true, true>() : kernel_ptr<SBR_PREC_FP32, false, true>();
-            return transposed ? kernel_ptr<SBR_PREC_FP32, true, false>() : kernel_ptr<SBR_PREC_FP32, false, false>();
-        default:
-            if (rec) return transposed ? kernel_ptr<SBR_PREC_FP64, true, true>() : kernel_ptr<SBR_PREC_FP64, false, true>();
-            return transposed ? kernel_ptr<SBR_PREC_FP64, true, false>() : kernel_ptr<SBR_PREC_FP64, false, false>();
+        case SBR_PREC_MIXED: return pick_epi_kernel<SBR_PREC_MIXED, false, false>(epi);
+        case SBR_PREC_FP32: return pick_epi_kernel<SBR_PREC_FP32, false, false>(epi);
+        default: return pick_epi_kernel<SBR_PREC_FP64, false, false>(epi);
     }
 }
 
@@ -607,9 +785,12 @@ void finalize(long long n_samples, int n_rep, const double* quantum, unsigned lo
 }  // namespace
 
 sbr_status plan_launch(sbr_plan* pl, bool records, sbr_ray_record* d_records) {
-    const bool transposed = pl->k_max > kRegK;
-    const void* fn = pick_kernel(pl->prec, transposed, records);
+    const bool pol = pl->pol == SBR_POL_HHVV && !records;
+    const int npol = pol ? 2 : 1;
+    const bool batched = pl->mode == SBR_MODE_BATCHED || records;
+    const void* fn = pick_kernel(pl->prec, (batched ? pl->k_max : 1) * npol, records, pol);
     TraceParams p{};
+    p.segpol = pl->d_segpol;
     p.S = pl->scene_view;
     p.segs = pl->d_segs;
     p.seg_item_base = pl->d_seg_base;
@@ -695,7 +876,7 @@ sbr_status plan_launch(sbr_plan* pl, bool records, sbr_ray_record* d_records) {
             }
         }
     }
-    finalize(pl->n_samples, kAccReplicas, pl->d_quantum, pl->d_acc, pl->d_field, (long long)pl->n_segs * 4,
+    finalize(pl->n_samples * npol, kAccReplicas, pl->d_quantum, pl->d_acc, pl->d_field, (long long)pl->n_segs * 4,
              pl->d_acc_stats, pl->d_stats, pl->d_queue, pl->n_samples + 1 + (long long)pl->chunks.size(), st);
     SBR_CUDA(cudaGetLastError());
     ++launches;
@@ -802,6 +983,8 @@ extern "C" sbr_status sbr_run_noalloc(sbr_scene* s, const sbr_job* job, double* 
     sbr_run_opts o{};
     if (opts) o = *opts;
     if (o.mode != SBR_MODE_BATCHED) return fail(SBR_ERR_UNSUPPORTED, "the allocation-free sweep runs batched only");
+    if (o.polarization != SBR_POL_SCALAR)
+        return fail(SBR_ERR_UNSUPPORTED, "the allocation-free sweep computes the scalar field only");
     sbr_status st = validate_run(s, job, 1, o);
     if (st != SBR_OK) return st;
     if (job->n_angles > SBR_NOALLOC_MAX_ANGLES)
@@ -840,7 +1023,7 @@ extern "C" sbr_status sbr_run_noalloc(sbr_scene* s, const sbr_job* job, double* 
     SBR_CUDA(cudaMemsetAsync(&D->queue, 0, sizeof(unsigned long long), stream));
 
     if (tot.n_items > 0) {
-        const void* fn = pick_kernel(o.precision, tot.k_max > kRegK, false);
+        const void* fn = pick_kernel(o.precision, tot.k_max, false, false);
         int resident = 0;
         st = resident_ctas(fn, o.ctas_per_sm, s->num_sms, &resident);
         if (st != SBR_OK) return st;

@@ -91,6 +91,15 @@ __device__ __forceinline__ float slab_f(float lx, float hx, float ly, float hy, 
     float tf = min3f(fmaxf(x0, x1), fmaxf(y0, y1), fminf(fmaxf(z0, z1), tMax));
     return tn <= tf * kSlabSlack ? tn : __int_as_float(0x7f800000);
 }
+// The same entry distance with the planes already ordered by the ray's direction
+// signs (near plane first on every axis): fma is monotone in the plane coordinate,
+// so this equals slab_f bit for bit without the six per-axis min / max.
+__device__ __forceinline__ float slab_nf(float nx, float fx, float ny, float fy, float nz, float fz, F3 inv, F3 oi,
+                                         float tMin, float tMax) {
+    const float tn = max3f(fmaf(nx, inv.x, -oi.x), fmaf(ny, inv.y, -oi.y), fmaxf(fmaf(nz, inv.z, -oi.z), tMin));
+    const float tf = min3f(fmaf(fx, inv.x, -oi.x), fmaf(fy, inv.y, -oi.y), fminf(fmaf(fz, inv.z, -oi.z), tMax));
+    return tn <= tf * kSlabSlack ? tn : __int_as_float(0x7f800000);
+}
 __device__ __forceinline__ double slab_d(double lx, double hx, double ly, double hy, double lz, double hz, D3 o,
                                          D3 inv, double tMin, double tMax) {
     double x0 = (lx - o.x) * inv.x, x1 = (hx - o.x) * inv.x;
@@ -194,11 +203,19 @@ struct Walker<false> {
                                                   uint32_t& err) {
         const F3 inv{slab_inv(d.x), slab_inv(d.y), slab_inv(d.z)};
         const F3 oi{o.x * inv.x, o.y * inv.y, o.z * inv.z};
+        // byte offsets of each axis' near and far planes within a GNode4 (lo planes
+        // at 0 / 32 / 64, hi planes 16 bytes after them): the ray's direction signs
+        // decide which plane enters a slab, so the loads pick the planes
+        const unsigned onx = inv.x < 0.0f ? 16u : 0u, ony = inv.y < 0.0f ? 48u : 32u, onz = inv.z < 0.0f ? 80u : 64u;
+        const unsigned ofx = onx ^ 16u, ofy = ony ^ 16u, ofz = onz ^ 16u;
         unsigned long long stack[kStackDepth];
         int sp = 0;
         int ref = 0;
         int best = -1;
         uint32_t iters = 0;
+        auto plane = [](const GNode4* p, unsigned off) {
+            return __ldg(reinterpret_cast<const float4*>(reinterpret_cast<const char*>(p) + off));
+        };
         auto push = [&](int r, float t) {
             if (sp < kStackDepth) stack[sp++] = pack_entry(r, t);
             else err |= DEV_ERR_STACK;
@@ -213,17 +230,26 @@ struct Walker<false> {
         for (;;) {
             while (ref >= 0) {
                 if (++iters > kIterBudget) { err |= DEV_ERR_BUDGET; return -1; }
-                const GNode4 n = load_node(S.nodes + ref);
-                float t[4] = {slab_f(n.lox.x, n.hix.x, n.loy.x, n.hiy.x, n.loz.x, n.hiz.x, inv, oi, tMin, tBest),
-                              slab_f(n.lox.y, n.hix.y, n.loy.y, n.hiy.y, n.loz.y, n.hiz.y, inv, oi, tMin, tBest),
-                              slab_f(n.lox.z, n.hix.z, n.loy.z, n.hiy.z, n.loz.z, n.hiz.z, inv, oi, tMin, tBest),
-                              slab_f(n.lox.w, n.hix.w, n.loy.w, n.hiy.w, n.loz.w, n.hiz.w, inv, oi, tMin, tBest)};
-                int c[4] = {n.child.x, n.child.y, n.child.z, n.child.w};
-                sort4(t, c);
-                if (t[0] <= tBest) {
+                const GNode4* np = S.nodes + ref;
+                const float4 nx = plane(np, onx), fx = plane(np, ofx), ny = plane(np, ony), fy = plane(np, ofy);
+                const float4 nz = plane(np, onz), fz = plane(np, ofz);
+                const int4 ch = __ldg(&np->child);
+                float t[4] = {slab_nf(nx.x, fx.x, ny.x, fy.x, nz.x, fz.x, inv, oi, tMin, tBest),
+                              slab_nf(nx.y, fx.y, ny.y, fy.y, nz.y, fz.y, inv, oi, tMin, tBest),
+                              slab_nf(nx.z, fx.z, ny.z, fy.z, nz.z, fz.z, inv, oi, tMin, tBest),
+                              slab_nf(nx.w, fx.w, ny.w, fy.w, nz.w, fz.w, inv, oi, tMin, tBest)};
+                int c[4] = {ch.x, ch.y, ch.z, ch.w};
+                // most visits accept exactly one child (no ordering needed); two or
+                // more are sorted and all but the nearest pushed, farthest first
+                const bool h0 = t[0] <= tBest, h1 = t[1] <= tBest, h2 = t[2] <= tBest, h3 = t[3] <= tBest;
+                const int nh = int(h0) + int(h1) + int(h2) + int(h3);
+                if (nh == 1) {
+                    ref = h0 ? c[0] : h1 ? c[1] : h2 ? c[2] : c[3];
+                } else if (nh > 1) {
+                    sort4(t, c);
                     if (t[3] <= tBest) push(c[3], t[3]);
                     if (t[2] <= tBest) push(c[2], t[2]);
-                    if (t[1] <= tBest) push(c[1], t[1]);
+                    push(c[1], t[1]);
                     ref = c[0];
                 } else if (!pop()) {
                     return best;
@@ -275,11 +301,17 @@ struct Walker<true> {
                                slab_d(n.lox.z, n.hix.z, n.loy.z, n.hiy.z, n.loz.z, n.hiz.z, o, inv, tMin, tBest),
                                slab_d(n.lox.w, n.hix.w, n.loy.w, n.hiy.w, n.loz.w, n.hiz.w, o, inv, tMin, tBest)};
                 int c[4] = {n.child.x, n.child.y, n.child.z, n.child.w};
-                sort4(t, c);
-                if (t[0] <= tBest) {
+                // most visits accept exactly one child (no ordering needed); two or
+                // more are sorted and all but the nearest pushed, farthest first
+                const bool h0 = t[0] <= tBest, h1 = t[1] <= tBest, h2 = t[2] <= tBest, h3 = t[3] <= tBest;
+                const int nh = int(h0) + int(h1) + int(h2) + int(h3);
+                if (nh == 1) {
+                    ref = h0 ? c[0] : h1 ? c[1] : h2 ? c[2] : c[3];
+                } else if (nh > 1) {
+                    sort4(t, c);
                     if (t[3] <= tBest) push(c[3], t[3]);
                     if (t[2] <= tBest) push(c[2], t[2]);
-                    if (t[1] <= tBest) push(c[1], t[1]);
+                    push(c[1], t[1]);
                     ref = c[0];
                 } else if (!pop()) {
                     return best;

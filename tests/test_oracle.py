@@ -120,3 +120,52 @@ def test_frame_is_orthogonal_and_matches_reference_layout(oracle):
         assert abs(np.dot(d, u)) < 1e-12 and abs(np.dot(d, v)) < 1e-12 and abs(np.dot(u, v)) < 1e-12
         np.testing.assert_allclose([np.linalg.norm(u), np.linalg.norm(v)], [2.0, 2.0], rtol=1e-12)
         np.testing.assert_allclose(f["llc"] + 0.5 * u + 0.5 * v, 20.0 * d, atol=1e-12)
+
+
+# ------------------------------------------------------------- polarised oracle
+# The polarised mode has no reference counterpart; its oracle is pinned to the
+# scalar oracle where the two must agree (single bounce) and to closed-form
+# physical-optics results where they differ (dihedral and trihedral returns).
+C0 = 299792458.0
+
+
+def test_pol_single_bounce_equals_scalar(oracle):
+    """Plate and sphere (single-bounce returns): HH == VV == the scalar field."""
+    for (v, t), th, ph, f, n, G in ((M.plate(1.0, 4), [0.0, 10.0, 20.0], [0.0, 30.0, 60.0], 3e9, 100, 1.5),
+                                    (M.icosphere(3), [90.0, 90.0], [0.0, 37.0], 1e9, 67, 2.0)):
+        s = oracle.sweep(v, t, th, ph, [f], n, n, G, 3).field[:, 0]
+        p = oracle.sweep_pol(v, t, th, ph, [f], n, n, G, 3)[:, 0, :]
+        tol = 1e-9 * np.abs(s).max()
+        assert np.all(np.abs(p[:, 0] - s) <= tol) and np.all(np.abs(p[:, 1] - s) <= tol)
+
+
+def test_pol_dihedral_broadside(oracle):
+    """90-degree dihedral, fold axis along z, seen at broadside (theta 90, phi 45):
+    double-bounce returns with HH = -VV and sigma = 8 pi a^2 b^2 / lambda^2
+    times cos^2(45 deg) (the ray-tube weighting cos(theta) of the exit term)."""
+    v, t = M.dihedral(1.0, 8)
+    f = 3e9
+    p = oracle.sweep_pol(v, t, [90.0], [45.0], [f], 120, 120, 2.0, 3)[0, 0]
+    ratio = p[0] / p[1]
+    assert abs(ratio + 1.0) < 2e-3, ratio
+    lam = C0 / f
+    want = 10 * np.log10(8 * np.pi / lam ** 2 * 0.5)
+    got = 10 * np.log10(4 * np.pi * np.abs(p) ** 2)
+    assert np.all(np.abs(got - want) < 0.3), (got, want)
+
+
+def test_pol_trihedral_boresight(oracle):
+    """Square trihedral at boresight: triple-bounce returns add in phase with the
+    physical exit path, HH = VV, sigma = 12 pi a^4 / lambda^2 times cos^2 = 1/3;
+    the scalar reference term (phase 2 k L) decoheres them."""
+    v, t = M.trihedral(1.0, 10)
+    f = 3e9
+    th0 = np.degrees(np.arccos(1 / np.sqrt(3)))
+    p = oracle.sweep_pol(v, t, [th0], [45.0], [f], 120, 120, np.sqrt(3), 3)[0, 0]
+    s = oracle.sweep(v, t, [th0], [45.0], [f], 120, 120, np.sqrt(3), 3).field[0, 0]
+    assert abs(p[0] / p[1] - 1.0) < 2e-3
+    lam = C0 / f
+    want = 10 * np.log10(12 * np.pi / lam ** 2 / 3)
+    got = 10 * np.log10(4 * np.pi * np.abs(p) ** 2)
+    assert np.all(np.abs(got - want) < 0.3), (got, want)
+    assert 10 * np.log10(4 * np.pi * abs(s) ** 2) < want - 30.0
