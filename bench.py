@@ -7,8 +7,11 @@ bounces, 2-D sweep theta = 0..90 x phi = 0..90 deg at 1 deg (8,281 angles), all
 drained by one persistent launch.  Other workloads (--workload): `sphere` (icosphere
 level 5, 1 GHz, 67^2 rays, 3 bounces, 360 azimuths), `aircraft` (seeded ~2.15 M
 triangle aircraft, 64 frequencies log-spaced over 1-18 GHz, 721 azimuths at 0.5 deg,
-5 bounces) and `aircraft-dev` (8 frequencies x 73 azimuths of the same).  All meshes
-are synthetic and seeded; no dataset is involved.
+5 bounces), `aircraft-dev` (8 frequencies x 73 azimuths of the same) and `ellipsoid`
+(the differentiable-shape case: ellipsoid 2/1/0.5 m with a seeded 32-mode spherical-
+harmonic displacement, 199,808 triangles, 5 GHz, G = 4 m, 668^2 rays, 4 bounces,
+121 azimuths over -30..30 deg; --adjoint also times the gradient of the mean RCS).
+All meshes are synthetic and seeded; no dataset is involved.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
 
@@ -73,10 +76,16 @@ def workload(name: str, rank: int = 0):
         ph = np.arange(0.0, 360.0 + 1e-9, step)
         th = np.full(ph.size, 90.0)
         freqs, mb = list(np.geomspace(1e9, 18e9, nf)), 5
+    elif name == "ellipsoid":
+        # differentiable-shape case: SH-displaced ellipsoid 2/1/0.5 m, 5 GHz, G = 4 m
+        v, t = M.ellipsoid_sh()
+        ph = np.arange(-30.0, 30.0 + 1e-9, 0.5)
+        th = np.full(ph.size, 90.0)
+        freqs, mb = [5e9], 4
     else:
         raise ValueError(name)
     ph = ph + 0.1 * rank
-    G = 2.0 * M.bounding_radius(v)
+    G = 4.0 if name == "ellipsoid" else 2.0 * M.bounding_radius(v)
     grid = {f: M.rays_for(f, G) for f in freqs}
     n = grid[max(freqs)]
     label = f"{name}_{t.shape[0]}tri_{len(freqs)}f_{min(freqs)/1e9:g}-{max(freqs)/1e9:g}GHz_{n}x{n}_{mb}b_{th.size}ang"
@@ -241,7 +250,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="trihedral", choices=["trihedral", "sphere", "aircraft", "aircraft-dev"])
+    ap.add_argument("--workload", default="trihedral", choices=["trihedral", "sphere", "aircraft", "aircraft-dev", "ellipsoid"])
+    ap.add_argument("--adjoint", action="store_true",
+                    help="also time the adjoint (gradient of the mean RCS w.r.t. vertices and frequency)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--angles", type=int, default=0,
                     help="profile case: trace only this many angles, evenly spread over the sweep")
@@ -374,6 +385,22 @@ def main():
                      "max_field_diff_vs_batched_rel_to_max": float(np.abs(pf - bf).max() / np.abs(bf).max())}
         pplan.close()
 
+    # reverse-mode gradient of mean(sigma) along the frozen hit paths (sbr_adjoint)
+    adj = None
+    if args.adjoint:
+        cot = 8.0 * np.pi * res.field / res.field.size
+        sbr.adjoint(scene, job, cot, precision=sbr.PREC_MIXED)  # warm-up
+        a_ms = []
+        for _ in range(max(1, min(args.steps, 3))):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            gx, gf = sbr.adjoint(scene, job, cot, precision=sbr.PREC_MIXED)
+            a_ms.append((time.perf_counter() - t0) * 1e3)
+        adj = {"ms": float(np.mean(a_ms)), "samples_per_s": samples / (float(np.mean(a_ms)) * 1e-3),
+               "rays_per_s": info["n_rays_clipped"] / (float(np.mean(a_ms)) * 1e-3),
+               "timing": "host wall clock around sbr_adjoint (host arrays in and out)",
+               "grad_norm": float(np.linalg.norm(gx)), "lit_vertices": int((np.abs(gx).sum(axis=1) > 0).sum())}
+
     # batched mixed precision against a full-FP64 run of the same batched job
     fp64 = None
     if args.fp64_check > 0:
@@ -435,6 +462,7 @@ def main():
         "kernel_ms": kern_ms,
         "per_angle": per_angle,
         "fp64_check": fp64,
+        "adjoint": adj,
         "e2e": {"value": e2e_value, "unit": "samples/s", "h2d_bytes_per_step": info["h2d_bytes"],
                 "d2h_bytes_per_step": info["d2h_bytes"], "ms_per_step": float(e2e_t[0])},
         "gpu_launches": int(info["launches_per_execute"]) * args.steps,

@@ -209,6 +209,26 @@ typedef struct sbr_ray_record {
 sbr_status sbr_trace_records(sbr_scene* scene, const sbr_job* job, const sbr_run_opts* opts,
                              sbr_ray_record* out);
 
+/* ----------------------------------------------------------------- adjoint */
+/* No counterpart in the reference (its sweep is not differentiable).
+ *
+ * Reverse-mode gradient of the scalar field sweep of `jobs` along the frozen hit
+ * paths: every ray is re-traced with the precision's own closest-hit walk, the
+ * path through the hit triangles is re-evaluated and differentiated in FP64, and
+ * hit / miss decisions and the cos > 0 gate are held fixed.
+ *   cot       [n_samples * 2]: complex cotangent g of every sample's field S, so
+ *             that dLoss = sum_s Re(conj(g_s) dS_s); for Loss = sum_s w_s sigma_s
+ *             it is g_s = 8 pi w_s S_s.
+ *   grad_xyz  [nverts * 3] out (may be NULL): dLoss / d(caller vertex coordinates)
+ *             (the unscaled xyz given to sbr_scene_create).
+ *   grad_freq [n_samples] out (may be NULL): dLoss / d(frequency in Hz) of each
+ *             sample's own term.
+ * Scalar polarisation only; at most 16 bounces and 128 frequencies per job; the
+ * mode option is ignored (one persistent launch).  Gradients are summed with FP64
+ * atomics, so their last bits vary from run to run. */
+sbr_status sbr_adjoint(sbr_scene* scene, const sbr_job* jobs, size_t n_jobs, const sbr_run_opts* opts,
+                       const double* cot, double* grad_xyz, double* grad_freq);
+
 /* ---------------------------------------------------- allocation-free sweep */
 /* No counterpart in the reference.
  *

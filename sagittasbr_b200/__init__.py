@@ -27,7 +27,7 @@ from ._lib import (FIRST_HIT_RASTER, FIRST_HIT_TRAVERSE, MODE_BATCHED, MODE_PER_
                    PREC_FP32, PREC_FP64, PREC_MIXED, SbrError, check, lib)
 
 __all__ = [
-    "Scene", "JobSpec", "SweepResult", "Plan", "run", "trace_records", "load_config", "config_angles",
+    "Scene", "JobSpec", "SweepResult", "Plan", "run", "adjoint", "trace_records", "load_config", "config_angles",
     "load_obj", "write_csv", "run_sweep", "SbrError", "MODE_BATCHED", "MODE_PER_ANGLE", "PREC_MIXED",
     "FIRST_HIT_RASTER", "FIRST_HIT_TRAVERSE",
     "PREC_FP32", "PREC_FP64", "POL_SCALAR", "POL_HHVV", "RAY_RECORD",
@@ -59,6 +59,7 @@ class Scene:
               "sbr_scene_create")
         self._h = h
         self.n_triangles = t.shape[0]
+        self.n_vertices = v.shape[0]
 
     @property
     def handle(self):
@@ -248,6 +249,28 @@ def run(scene: Scene, jobs: Sequence[JobSpec] | JobSpec, mode=MODE_BATCHED, prec
               first_hit=FIRST_HIT_TRAVERSE if first_hit is None else first_hit)
     check(lib().sbr_run(scene.handle, jc, len(jobs), C.byref(r), C.byref(o)), "sbr_run")
     return _result(f, s, d, st.reshape(na, 4), r.device_ms, npol)
+
+
+def adjoint(scene: Scene, jobs: Sequence[JobSpec] | JobSpec, cot, precision=PREC_MIXED):
+    """sbr_adjoint: gradient of a loss of the sweep's fields along the frozen hit paths.
+
+    cot: complex [n_samples] cotangent g of each sample's field S (dLoss =
+    sum Re(conj(g) dS)).  Returns (grad_xyz [nverts, 3] with respect to the caller's
+    vertex coordinates, grad_freq [n_samples] with respect to each sample's
+    frequency in Hz)."""
+    if isinstance(jobs, JobSpec):
+        jobs = [jobs]
+    jc = _jobs_c(jobs)
+    n = sum(j.n_angles * j.n_freqs for j in jobs)
+    g = np.ascontiguousarray(np.asarray(cot, dtype=np.complex128).ravel())
+    if g.size != n:
+        raise ValueError(f"cotangent has {g.size} entries, the jobs have {n} samples")
+    c2 = np.ascontiguousarray(np.stack([g.real, g.imag], axis=1).ravel())
+    gx = np.zeros(3 * scene.n_vertices)
+    gf = np.zeros(n)
+    o = _opts(MODE_BATCHED, precision)
+    check(lib().sbr_adjoint(scene.handle, jc, len(jobs), C.byref(o), _p(c2), _p(gx), _p(gf)), "sbr_adjoint")
+    return gx.reshape(-1, 3), gf
 
 
 def trace_records(scene: Scene, job: JobSpec, precision=PREC_MIXED, first_hit=None) -> np.ndarray:

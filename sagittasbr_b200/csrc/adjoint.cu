@@ -1,0 +1,340 @@
+// adjoint.cu -- reverse-mode gradient of the scalar PO field sweep with respect to
+// the mesh vertices and the frequency, along frozen hit paths (sm_100a).
+// No counterpart in the reference, whose sweep is not differentiable.
+//
+// For every ray of every (angle, frequency) sample the kernel
+//   1. re-traces the ray with the precision's own closest-hit walk (the same
+//      start_f / step_f or start_d / step_d as the sweep kernel) and keeps the ids
+//      of the triangles it hits -- the path is recomputed, nothing is stored in HBM;
+//   2. re-evaluates that path in FP64 from the caller's vertices: per bounce the
+//      ray-plane distance t = ((a - o).N) / (d.N) of the hit triangle (N = e1 x e2),
+//      the hit point, the unit normal, the reflected direction and the nudged
+//      origin (src/cuda/rtKernels.cu:126-158), then the exit term
+//      T_k = k A / (4 pi) * 2 cos R^n * j exp(j 2 k L)   (src/cuda/poKernels.cu:81-109);
+//   3. runs the chain rule backwards through the bounces, seeded by the caller's
+//      cotangent g_k of each sample's field (dLoss = sum Re(conj(g_k) dS_k)), and
+//      adds the vertex adjoints to the gradient with FP64 atomics.
+// Hit / miss decisions and the cos > 0 gate are held fixed (the gradient of the
+// smooth part; edge crossings are not differentiated).
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "plan.hpp"
+#include "ray.cuh"
+
+namespace sbr {
+namespace {
+
+constexpr int kAdjMaxBounces = SBR_MAX_REC;
+constexpr int kAdjMaxK = 128;
+
+struct AdjointParams {
+    SceneView S;
+    const float* xyz;              // caller vertices (unscaled), [nverts * 3]
+    const uint32_t* idx;           // caller triangles, [ntris * 3]
+    double model_scale;
+    const Segment* segs;
+    const int64_t* seg_item_base;  // [n_segs + 1]
+    int32_t n_segs;
+    const JobConst* jobs;
+    const FreqConst* freqs;
+    int64_t n_items;
+    unsigned long long* queue;
+    const double* cot;             // [n_samples][2] cotangents of the fields
+    double* grad_pos;              // [nverts * 3] dLoss / d(scaled vertex position)
+    double* grad_k;                // [n_samples] dLoss / dk
+    uint32_t* err;
+    const volatile int32_t* cancel;
+};
+
+__device__ __forceinline__ D3 vertex(const AdjointParams& P, uint32_t v) {
+    return D3{double(__ldg(P.xyz + 3 * v)) * P.model_scale, double(__ldg(P.xyz + 3 * v + 1)) * P.model_scale,
+              double(__ldg(P.xyz + 3 * v + 2)) * P.model_scale};
+}
+
+__device__ __forceinline__ void scatter(double* g, uint32_t v, D3 a) {
+    atomicAdd(g + 3 * v, a.x);
+    atomicAdd(g + 3 * v + 1, a.y);
+    atomicAdd(g + 3 * v + 2, a.z);
+}
+
+// One ray: frozen path, FP64 re-evaluation, reverse sweep.  Frequency adjoints are
+// added to the lane's own row gk[0..K).
+template <int PREC>
+__device__ void adjoint_ray(const AdjointParams& P, const Segment& G, const JobConst& J, const FreqConst* F, int K,
+                            const double* cot, int i, int j, double* gk, uint32_t& err) {
+    // 1. the precision's own hit sequence (caller triangle ids)
+    sbr_ray_record rec;
+    int n = 0;
+    if (PREC == SBR_PREC_FP64) {
+        RayD r;
+        PolD e;
+        start_d(r, G, J, i, j);
+        if (J.max_bounces > 0)
+            while (!step_d<true, false>(r, e, P.S, J.max_bounces, err, &rec)) {}
+        n = r.count;
+    } else {
+        RayF r;
+        PolF e;
+        start_f<PREC>(r, G, J, i, j);
+        if (J.max_bounces > 0)
+            while (!step_f<PREC, true, false>(r, e, P.S, J.max_bounces, err, &rec, nullptr)) {}
+        n = r.count;
+    }
+    if (n == 0) return;
+
+    // 2. FP64 forward along the frozen path
+    double oS[kAdjMaxBounces][3], dS[kAdjMaxBounces][3], tS[kAdjMaxBounces];
+    D3 o{G.llc[0] + (double(i) + 0.5) / double(J.nx) * G.u[0] + (double(j) + 0.5) / double(J.ny) * G.v[0],
+         G.llc[1] + (double(i) + 0.5) / double(J.nx) * G.u[1] + (double(j) + 0.5) / double(J.ny) * G.v[1],
+         G.llc[2] + (double(i) + 0.5) / double(J.nx) * G.u[2] + (double(j) + 0.5) / double(J.ny) * G.v[2]};
+    D3 d{-G.dir[0], -G.dir[1], -G.dir[2]};
+    double L = G.shift;
+    D3 nLast{0, 0, 0}, dLast{0, 0, 0};
+    for (int b = 0; b < n; ++b) {
+        const int tri = rec.tri[b];
+        const D3 a = vertex(P, __ldg(P.idx + 3 * tri)), bb = vertex(P, __ldg(P.idx + 3 * tri + 1)),
+                 c = vertex(P, __ldg(P.idx + 3 * tri + 2));
+        const D3 N = cross(bb - a, c - a);
+        const double t = dot(a - o, N) / dot(d, N);
+        oS[b][0] = o.x; oS[b][1] = o.y; oS[b][2] = o.z;
+        dS[b][0] = d.x; dS[b][1] = d.y; dS[b][2] = d.z;
+        tS[b] = t;
+        const D3 nn = unit(N);
+        nLast = nn;
+        dLast = d;
+        L += t;
+        const D3 p = o + t * d;
+        d = unit(d - (2.0 * dot(d, nn)) * nn);
+        o = p + 1.0e-4 * nn;
+    }
+    const double cosT = -dot(nLast, dLast);
+    if (!(cosT > 0.0)) return;  // the scalar gate: no term, no gradient
+    double Rn = 1.0;
+    for (int b = 0; b < n; ++b) Rn *= J.refl;
+
+    // exit-term adjoints: w_c = dLoss/dcos, w_L = dLoss/dL; per frequency dLoss/dk
+    double wc = 0.0, wL = 0.0;
+    for (int k = 0; k < K; ++k) {
+        const double gr = __ldg(cot + 2 * k), gi = __ldg(cot + 2 * k + 1);
+        if (gr == 0.0 && gi == 0.0) continue;
+        const double x = F[k].turns * L;  // 2 k L in turns
+        double s, c;
+        sincospi(2.0 * (x - rint(x)), &s, &c);
+        const double A = 2.0 * F[k].scale * Rn;  // |T_k| / cos
+        const double Pk = -gr * s + gi * c;       // Re(conj(g) j e^{j phi})
+        const double Qk = gr * c + gi * s;        // Im(conj(g) j e^{j phi})
+        wc += A * Pk;
+        wL -= 2.0 * F[k].k * A * cosT * Qk;
+        gk[k] += A * cosT * (Pk / F[k].k - 2.0 * L * Qk);
+    }
+
+    // 3. reverse sweep over the bounces
+    D3 ob{0, 0, 0}, db{0, 0, 0};  // adjoints of the origin / direction after bounce b
+    for (int b = n - 1; b >= 0; --b) {
+        const int tri = rec.tri[b];
+        const uint32_t ia = __ldg(P.idx + 3 * tri), ib = __ldg(P.idx + 3 * tri + 1), ic = __ldg(P.idx + 3 * tri + 2);
+        const D3 a = vertex(P, ia), e1 = vertex(P, ib) - a, e2 = vertex(P, ic) - a;
+        const D3 N = cross(e1, e2);
+        const double lenN = sqrt(dot(N, N));
+        const D3 nn = (1.0 / lenN) * N;
+        const D3 ov{oS[b][0], oS[b][1], oS[b][2]}, dv{dS[b][0], dS[b][1], dS[b][2]};
+        const double t = tS[b];
+
+        D3 nb{0, 0, 0};
+        D3 dbar{0, 0, 0};
+        double tb = wL;
+        if (b == n - 1) {  // cos = -nn.d
+            nb = nb - wc * dv;
+            dbar = dbar - wc * nn;
+        }
+        // o_{b+1} = p + 1e-4 nn
+        const D3 pb = ob;
+        nb = nb + 1.0e-4 * ob;
+        // d_{b+1} = d - 2 (d.nn) nn   (unit length is preserved, so unit() adds nothing)
+        const double dn = dot(dv, nn), ndb = dot(nn, db);
+        dbar = dbar + db - (2.0 * ndb) * nn;
+        nb = nb - 2.0 * (dn * db + ndb * dv);
+        // p = o + t d
+        D3 obar = pb;
+        tb += dot(pb, dv);
+        dbar = dbar + t * pb;
+        // t = ((a - o).N) / (d.N)
+        const double den = dot(dv, N);
+        const double numb = tb / den, denb = -tb * t / den;
+        D3 ab = numb * N;
+        obar = obar - numb * N;
+        D3 Nb = numb * (a - ov) + denb * dv;
+        dbar = dbar + denb * N;
+        // nn = N / |N|
+        Nb = Nb + (1.0 / lenN) * (nb - dot(nb, nn) * nn);
+        // N = e1 x e2, e1 = v1 - a, e2 = v2 - a
+        const D3 e1b = cross(e2, Nb), e2b = cross(Nb, e1);
+        ab = ab - (e1b + e2b);
+        scatter(P.grad_pos, ia, ab);
+        scatter(P.grad_pos, ib, e1b);
+        scatter(P.grad_pos, ic, e2b);
+        ob = obar;
+        db = dbar;
+    }
+}
+
+template <int PREC>
+__global__ void __launch_bounds__(kCtaThreads) k_adjoint(const AdjointParams P) {
+    constexpr unsigned FULL = 0xffffffffu;
+    double gk[kAdjMaxK];  // this lane's dLoss/dk of the current item (local memory)
+    const int lane = threadIdx.x & 31;
+    uint32_t err = 0;
+    int iter = 0;
+    for (;;) {
+        long long item = 0;
+        if (lane == 0) {
+            item = (long long)atomicAdd(P.queue, 1ull);
+            if (item < P.n_items && P.cancel && (iter & 15) == 0 && *P.cancel != 0) {
+                atomicOr(P.err, DEV_ERR_CANCEL);
+                item = P.n_items;
+            }
+        }
+        item = __shfl_sync(FULL, item, 0);
+        if (item >= P.n_items) break;
+        ++iter;
+        const int seg = find_segment(P.seg_item_base, P.n_segs, item);
+        const Segment& G = P.segs[seg];
+        const JobConst J = P.jobs[G.job];
+        const int K = J.n_freqs;
+        const FreqConst* F = P.freqs + J.freq_base;
+        const double* cot = P.cot + 2 * G.sample_base;
+        for (int k = 0; k < K; ++k) gk[k] = 0.0;
+        const int b0 = int(item - G.item_base) * G.blocks_per_item;
+        const int nslots = min(G.blocks_per_item, G.blocks - b0) * 32;
+        for (int s = lane; s < nslots; s += 32) {
+            const int blk = b0 + (s >> 5), l = s & 31;
+            const int i = G.i0 + (blk % G.blocks_x) * kBlockW + (l & 7);
+            const int j = G.j0 + (blk / G.blocks_x) * kBlockH + (l >> 3);
+            if (i < G.i0 + G.ni && j < G.j0 + G.nj) adjoint_ray<PREC>(P, G, J, F, K, cot, i, j, gk, err);
+        }
+        // lanes -> warp in a fixed order, one atomic per (item, frequency)
+        for (int k = 0; k < K; ++k) {
+            double v = gk[k];
+            for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(FULL, v, off);
+            if (lane == 0 && v != 0.0) atomicAdd(P.grad_k + G.sample_base + k, v);
+        }
+    }
+    if (err) atomicOr(P.err, err);
+}
+
+const void* pick_adjoint(int prec) {
+    switch (prec) {
+        case SBR_PREC_MIXED: return reinterpret_cast<const void*>(&k_adjoint<SBR_PREC_MIXED>);
+        case SBR_PREC_FP32: return reinterpret_cast<const void*>(&k_adjoint<SBR_PREC_FP32>);
+        default: return reinterpret_cast<const void*>(&k_adjoint<SBR_PREC_FP64>);
+    }
+}
+
+// Device buffers of one adjoint call, released on every exit path.
+struct AdjointBuffers {
+    double* cot = nullptr;
+    double* grad_pos = nullptr;
+    double* grad_k = nullptr;
+    ~AdjointBuffers() {
+        cudaFree(cot);
+        cudaFree(grad_pos);
+        cudaFree(grad_k);
+    }
+};
+
+}  // namespace
+
+// Caller vertices and triangles on the device (uploaded once per scene).
+sbr_status ensure_adjoint_data(sbr_scene* s) {
+    if (s->d_xyz && s->d_idx) return SBR_OK;
+    SBR_CUDA(cudaSetDevice(s->device));
+    const size_t vb = s->xyz.size() * sizeof(float), ib = s->idx.size() * sizeof(uint32_t);
+    if (cudaMalloc(&s->d_xyz, vb) != cudaSuccess || cudaMalloc(&s->d_idx, ib) != cudaSuccess)
+        return fail(SBR_ERR_OOM, "cudaMalloc of the adjoint mesh copy failed");
+    SBR_CUDA(cudaMemcpy(s->d_xyz, s->xyz.data(), vb, cudaMemcpyHostToDevice));
+    SBR_CUDA(cudaMemcpy(s->d_idx, s->idx.data(), ib, cudaMemcpyHostToDevice));
+    s->device_bytes += (int64_t)(vb + ib);
+    return SBR_OK;
+}
+
+}  // namespace sbr
+
+extern "C" sbr_status sbr_adjoint(sbr_scene* s, const sbr_job* jobs, size_t n_jobs, const sbr_run_opts* opts,
+                                  const double* cot, double* grad_xyz, double* grad_freq) {
+    using namespace sbr;
+    if (!s || !cot) return fail(SBR_ERR_INVALID_ARG, "scene and cotangents are required");
+    sbr_run_opts o{};
+    if (opts) o = *opts;
+    if (o.polarization != SBR_POL_SCALAR) return fail(SBR_ERR_UNSUPPORTED, "the adjoint covers the scalar field");
+    for (size_t k = 0; k < n_jobs; ++k)
+        if (jobs && jobs[k].max_bounces > kAdjMaxBounces)
+            return fail(SBR_ERR_TOO_LARGE, "the adjoint follows at most 16 bounces");
+    o.mode = SBR_MODE_BATCHED;
+    o.first_hit = SBR_FIRST_HIT_TRAVERSE;
+    o.use_graph = 0;
+    sbr_plan* p = nullptr;
+    sbr_status st = sbr_plan_create(s, jobs, n_jobs, &o, &p);
+    if (st != SBR_OK) return st;
+    struct PlanGuard {
+        sbr_plan* p;
+        ~PlanGuard() { sbr_plan_destroy(p); }
+    } guard{p};
+    for (int64_t g = 0; g < p->n_segs; ++g)
+        if (p->jobs[p->segs[g].job].n_freqs > kAdjMaxK) return fail(SBR_ERR_TOO_LARGE, "more than 128 frequencies");
+    if ((st = ensure_adjoint_data(s)) != SBR_OK) return st;
+
+    const size_t nv3 = s->xyz.size(), ns = (size_t)p->n_samples;
+    AdjointBuffers B;
+    cudaStream_t stream = p->stream;
+    if (cudaMalloc(&B.cot, std::max<size_t>(1, 2 * ns) * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&B.grad_pos, nv3 * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&B.grad_k, std::max<size_t>(1, ns) * sizeof(double)) != cudaSuccess)
+        return fail(SBR_ERR_OOM, "adjoint buffers");
+    if (ns) SBR_CUDA(cudaMemcpyAsync(B.cot, cot, 2 * ns * sizeof(double), cudaMemcpyHostToDevice, stream));
+    SBR_CUDA(cudaMemsetAsync(B.grad_pos, 0, nv3 * sizeof(double), stream));
+    SBR_CUDA(cudaMemsetAsync(B.grad_k, 0, std::max<size_t>(1, ns) * sizeof(double), stream));
+
+    if (p->n_items > 0) {
+        const void* fn = pick_adjoint(p->prec);
+        int occ = 0;
+        SBR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kCtaThreads, 0));
+        const long long grid = std::min<long long>((long long)std::max(1, occ) * s->num_sms, (p->n_items + 3) / 4);
+        AdjointParams a{};
+        a.S = p->scene_view;
+        a.xyz = s->d_xyz;
+        a.idx = s->d_idx;
+        a.model_scale = s->model_scale;
+        a.segs = p->d_segs;
+        a.seg_item_base = p->d_seg_base;
+        a.n_segs = (int32_t)p->n_segs;
+        a.jobs = p->d_jobs;
+        a.freqs = p->d_freqs;
+        a.n_items = p->n_items;
+        a.queue = p->d_queue;
+        a.cot = B.cot;
+        a.grad_pos = B.grad_pos;
+        a.grad_k = B.grad_k;
+        a.err = s->d_err;
+        a.cancel = s->d_cancel;
+        void* args[] = {&a};
+        SBR_CUDA(cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(kCtaThreads), args, 0, stream));
+    }
+    std::vector<double> gp(nv3), gk(ns);
+    SBR_CUDA(cudaMemcpyAsync(gp.data(), B.grad_pos, nv3 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    if (ns) SBR_CUDA(cudaMemcpyAsync(gk.data(), B.grad_k, ns * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    SBR_CUDA(cudaStreamSynchronize(stream));
+    uint32_t e = 0;
+    SBR_CUDA(cudaMemcpy(&e, s->d_err, sizeof(e), cudaMemcpyDeviceToHost));
+    if (e) SBR_CUDA(cudaMemset(s->d_err, 0, sizeof(e)));
+    if (e & DEV_ERR_CANCEL) return fail(SBR_ERR_CANCELLED, "run cancelled");
+    if (e & DEV_ERR_BUDGET) return fail(SBR_ERR_TIMEOUT, "traversal iteration budget exceeded");
+    if (e & DEV_ERR_STACK) return fail(SBR_ERR_STACK, "traversal stack overflow");
+    // positions are model_scale * caller coordinates; k = 2 pi f / c
+    if (grad_xyz)
+        for (size_t q = 0; q < nv3; ++q) grad_xyz[q] = gp[q] * s->model_scale;
+    if (grad_freq)
+        for (size_t q = 0; q < ns; ++q) grad_freq[q] = gk[q] * (2.0 * M_PI / 299792458.0);
+    return SBR_OK;
+}

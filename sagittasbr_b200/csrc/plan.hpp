@@ -26,6 +26,8 @@ struct sbr_scene {
     sbr::GTri* d_tris = nullptr;
     sbr::GTri64* d_tris64 = nullptr;
     int32_t* d_tri_id = nullptr;
+    float* d_xyz = nullptr;          // caller vertices and triangles, uploaded for the adjoint
+    uint32_t* d_idx = nullptr;
     uint32_t* d_err = nullptr;
     int32_t* d_cancel = nullptr;     // device word polled by the kernels
     int32_t* h_flag_vals = nullptr;  // pinned {1, 0}: sources of the async flag copies
@@ -120,4 +122,5 @@ sbr_status plan_launch(sbr_plan* pl, bool records, sbr_ray_record* d_records);
 sbr_status fill_records(sbr_ray_record* d, long long n, cudaStream_t st);
 int max_freqs_per_job();
 sbr_status ensure_fp64(sbr_scene* s);
+sbr_status ensure_adjoint_data(sbr_scene* s);
 }  // namespace sbr

@@ -1,0 +1,205 @@
+// ray.cuh -- per-ray state of the SBR bounce loop on sm_100a, shared by the sweep
+// kernel (trace.cu) and the adjoint kernel (adjoint.cu): primary ray origins, one
+// closest-hit query with PEC reflection and nudge, and the scalar exit-ray
+// quantities of the PO term (src/cuda/rtKernels.cu:105-158,
+// src/cuda/poKernels.cu:81-109).
+#pragma once
+
+#include "trace.cuh"
+
+namespace sbr {
+
+// State of one ray between closest-hit queries.
+struct RayF {
+    F3 o, d, nl, dl;
+    double L;       // FP64 path (mixed)
+    float dist32;   // FP32 path (reference FP32 arithmetic)
+    int count;
+    int zidx;       // entry of this ray in the first-hit buffer
+};
+struct RayD {
+    D3 o, d, nl, dl;
+    double L;
+    int count;
+};
+
+// What the PO epilogue needs from a finished ray.
+struct RayOut {
+    float amp;     // 2 cos(theta) R^n, 0 when the ray adds nothing
+    float dist32;
+    double L;
+    float cosT, Rn;
+    double cosD, RnD;
+    double pa[2];  // SBR_POL_HHVV: co-polarised amplitudes (HH, VV)
+    double Lp;     // SBR_POL_HHVV: path launch plane -> exit point -> launch plane
+};
+
+// Polarisation state of SBR_POL_HHVV plans: the HH and VV incident fields as they
+// arrive at the ray's latest hit (unit vectors; PEC reflection keeps them real).
+struct PolF {
+    F3 h, v;
+};
+struct PolD {
+    D3 h, v;
+};
+
+// PEC boundary condition: the reflected field is 2 (n.E) n - E (tangential part
+// reversed, normal part kept).
+__device__ __forceinline__ F3 pec_reflect(F3 e, F3 n) {
+    const float s = 2.0f * dot(n, e);
+    return f3(s * n.x - e.x, s * n.y - e.y, s * n.z - e.z);
+}
+__device__ __forceinline__ D3 pec_reflect(D3 e, D3 n) {
+    const double s = 2.0 * dot(n, e);
+    return D3{s * n.x - e.x, s * n.y - e.y, s * n.z - e.z};
+}
+
+// Co-polarised exit amplitude: 2 R^n e.(n x (d_in x E_in)), the direction of the PO
+// surface current n x H_in on the last surface projected on the receive
+// polarisation e, with the scalar term's ray-tube weighting.  For a single bounce
+// (E_in = e, d_in = -s) it equals the scalar amplitude 2 cos(theta) R^n.
+template <class V, class R>
+__device__ __forceinline__ R pol_amp(V e, V n, V d, V E, R twoRn) {
+    return twoRn * dot(e, cross(n, cross(d, E)));
+}
+
+// ------------------------------------------------------------ FP32 / mixed
+// Origin of the primary ray of pixel (i, j) (src/cuda/rtKernels.cu:120-123); the
+// trace and the first-hit raster both use this, so they test identical rays.
+template <int PREC>
+__device__ __forceinline__ F3 primary_origin(const Segment& G, const JobConst& J, int i, int j) {
+    if (PREC == SBR_PREC_FP32) {
+        const float u = __fdiv_rn(float(i) + 0.5f, float(J.nx));
+        const float v = __fdiv_rn(float(j) + 0.5f, float(J.ny));
+        return f3(G.llcf[0] + u * G.uf[0] + v * G.vf[0], G.llcf[1] + u * G.uf[1] + v * G.vf[1],
+                  G.llcf[2] + u * G.uf[2] + v * G.vf[2]);
+    } else {
+        const double u = (double(i) + 0.5) * J.inv_nx;
+        const double v = (double(j) + 0.5) * J.inv_ny;
+        return f3(float(G.llc[0] + u * G.u[0] + v * G.v[0]), float(G.llc[1] + u * G.u[1] + v * G.v[1]),
+                  float(G.llc[2] + u * G.u[2] + v * G.v[2]));
+    }
+}
+
+template <int PREC>
+__device__ __forceinline__ void start_f(RayF& r, const Segment& G, const JobConst& J, int i, int j) {
+    r.o = primary_origin<PREC>(G, J, i, j);
+    r.L = PREC == SBR_PREC_FP32 ? 0.0 : G.shift;
+    r.zidx = (int)(G.zbase + (int64_t)(j - G.j0) * G.ni + (i - G.i0));
+    r.d = f3(G.rdf[0], G.rdf[1], G.rdf[2]);
+    r.nl = f3(0, 0, 0);
+    r.dl = f3(0, 0, 0);
+    r.dist32 = 0.0f;
+    r.count = 0;
+}
+
+// One closest-hit query, then reflect and nudge; true when the ray is finished.
+// The first query is read from the first-hit buffer when there is one (and the
+// entry is restored to empty for the next chunk).
+template <int PREC, bool REC, bool POL>
+__device__ __forceinline__ bool step_f(RayF& r, PolF& e, const SceneView& S, int maxB, uint32_t& err,
+                                       sbr_ray_record* rec, unsigned long long* zbuf) {
+    float tB = 1e20f;
+    int slot;
+    if (zbuf != nullptr && r.count == 0) {
+        const unsigned long long key = zbuf[r.zidx];
+        zbuf[r.zidx] = ~0ull;
+        if (key == ~0ull) return true;
+        tB = __uint_as_float((unsigned)(key >> 32));
+        slot = (int)(unsigned)key;
+    } else {
+        slot = Walker<false>::closest(S, r.o, r.d, 1.0e-3f, tB, err);
+    }
+    if (slot < 0) return true;
+    const GTri* T = S.tris + slot;
+    const F3 n = f3(__ldg(&T->p.w), __ldg(&T->e1.w), __ldg(&T->e2.w));
+    if constexpr (POL) {
+        if (r.count > 0) {  // the field left the previous hit reflected there
+            e.h = pec_reflect(e.h, r.nl);
+            e.v = pec_reflect(e.v, r.nl);
+        }
+    }
+    r.nl = n;
+    r.dl = r.d;
+    ++r.count;
+    if (PREC == SBR_PREC_FP32) r.dist32 += tB;
+    else r.L += double(tB);
+    if (REC && r.count <= SBR_MAX_REC) rec->tri[r.count - 1] = __ldg(S.tri_id + slot);
+    const F3 p = r.o + tB * r.d;
+    const float dn = 2.0f * dot(r.d, n);
+    r.d = unit(r.d - dn * n);
+    r.o = p + 1.0e-4f * n;
+    return r.count >= maxB;
+}
+
+template <int PREC>
+__device__ __forceinline__ RayOut finish_f(const RayF& r, const JobConst& J) {
+    RayOut o;
+    float Rn = 1.0f;
+    for (int b = 0; b < r.count; ++b) Rn *= J.reflf;
+    const float c = dot(r.nl, f3(-r.dl.x, -r.dl.y, -r.dl.z));
+    o.cosT = c;
+    o.Rn = Rn;
+    o.cosD = c;
+    o.RnD = Rn;
+    o.dist32 = r.dist32;
+    o.L = (PREC == SBR_PREC_FP32) ? double(r.dist32) : r.L;
+    o.amp = (r.count > 0 && c > 0.0f) ? 2.0f * c * Rn : 0.0f;
+    return o;
+}
+
+// --------------------------------------------------------------------- FP64
+__device__ __forceinline__ void start_d(RayD& r, const Segment& G, const JobConst& J, int i, int j) {
+    const double u = (double(i) + 0.5) / double(J.nx);
+    const double v = (double(j) + 0.5) / double(J.ny);
+    r.o = D3{G.llc[0] + u * G.u[0] + v * G.v[0], G.llc[1] + u * G.u[1] + v * G.v[1],
+             G.llc[2] + u * G.u[2] + v * G.v[2]};
+    r.d = D3{-G.dir[0], -G.dir[1], -G.dir[2]};
+    r.nl = D3{0, 0, 0};
+    r.dl = D3{0, 0, 0};
+    r.L = G.shift;
+    r.count = 0;
+}
+
+template <bool REC, bool POL>
+__device__ __forceinline__ bool step_d(RayD& r, PolD& e, const SceneView& S, int maxB, uint32_t& err,
+                                       sbr_ray_record* rec) {
+    double tB = 1e20;
+    const int slot = Walker<true>::closest(S, r.o, r.d, 1.0e-3, tB, err);
+    if (slot < 0) return true;
+    const GTri64& T = S.tris64[slot];
+    const D3 n{T.n[0], T.n[1], T.n[2]};
+    if constexpr (POL) {
+        if (r.count > 0) {
+            e.h = pec_reflect(e.h, r.nl);
+            e.v = pec_reflect(e.v, r.nl);
+        }
+    }
+    r.nl = n;
+    r.dl = r.d;
+    ++r.count;
+    r.L += tB;
+    if (REC && r.count <= SBR_MAX_REC) rec->tri[r.count - 1] = __ldg(S.tri_id + slot);
+    const D3 p = r.o + tB * r.d;
+    const double dn = 2.0 * dot(r.d, n);
+    r.d = unit(r.d - dn * n);
+    r.o = p + 1.0e-4 * n;
+    return r.count >= maxB;
+}
+
+__device__ __forceinline__ RayOut finish_d(const RayD& r, const JobConst& J) {
+    RayOut o;
+    double Rn = 1.0;
+    for (int b = 0; b < r.count; ++b) Rn *= J.refl;
+    const double c = dot(r.nl, D3{-r.dl.x, -r.dl.y, -r.dl.z});
+    o.cosT = float(c);
+    o.Rn = float(Rn);
+    o.cosD = c;
+    o.RnD = Rn;
+    o.L = r.L;
+    o.dist32 = float(r.L);
+    o.amp = (r.count > 0 && c > 0.0) ? float(2.0 * c * Rn) : 0.0f;
+    return o;
+}
+
+}  // namespace sbr

@@ -46,6 +46,8 @@ void free_scene(sbr_scene* s) {
     cudaFree(s->d_tris);
     cudaFree(s->d_tris64);
     cudaFree(s->d_tri_id);
+    cudaFree(s->d_xyz);
+    cudaFree(s->d_idx);
     cudaFree(s->d_err);
     cudaFree(s->d_cancel);
     if (s->h_flag_vals) cudaFreeHost(s->h_flag_vals);

@@ -331,4 +331,15 @@ struct Walker<true> {
     }
 };
 
+// Segment owning a work item: base[] holds each segment's first item (ascending).
+__device__ __forceinline__ int find_segment(const int64_t* base, int n, int64_t item) {
+    int lo = 0, hi = n;  // base[lo] <= item < base[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(base + mid) <= item) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
 }  // namespace sbr

@@ -267,6 +267,52 @@ def aircraft(seed: int = 1, jitter: float = 1e-3, fuselage=(1000, 600), wing=(10
     return centre_on_aabb(V), T.astype(np.uint32)
 
 
+def real_sph_harm(l: int, m: int, theta, phi):
+    """Orthonormal real spherical harmonic Y_lm (theta polar from +z, phi azimuth)."""
+    from scipy.special import lpmv
+    am = abs(m)
+    norm = math.sqrt((2 * l + 1) / (4 * math.pi) * math.factorial(l - am) / math.factorial(l + am))
+    p = lpmv(am, l, np.cos(theta))
+    if m == 0:
+        return norm * p
+    return math.sqrt(2.0) * norm * p * (np.cos(am * phi) if m > 0 else np.sin(am * phi))
+
+
+def ellipsoid_sh(axes=(2.0, 1.0, 0.5), n_theta: int = 224, n_phi: int = 448, n_modes: int = 32,
+                 sigma: float = 0.01, seed: int = 4):
+    """Ellipsoid with the given semi-axes, tessellated on a (theta, phi) grid
+    (2 n_phi (n_theta - 1) triangles: 199,808 at the defaults), each vertex moved
+    radially by a seeded field sum_i a_i Y_i(theta, phi) over the first ``n_modes``
+    real spherical harmonics (l = 0, 1, ...; m = -l..l), a_i ~ N(0, sigma) metres."""
+    rng = np.random.default_rng(seed)
+    modes = [(l, m) for l in range(16) for m in range(-l, l + 1)][:n_modes]
+    amps = rng.normal(0.0, sigma, size=len(modes))
+    th = np.linspace(0.0, np.pi, n_theta + 1)[1:-1]
+    ph = np.linspace(0.0, 2 * np.pi, n_phi, endpoint=False)
+    TH, PH = np.meshgrid(th, ph, indexing="ij")
+    a, b, c = axes
+    P = np.stack([a * np.sin(TH) * np.cos(PH), b * np.sin(TH) * np.sin(PH), c * np.cos(TH)], axis=-1)
+    delta = sum(amp * real_sph_harm(l, m, TH, PH) for amp, (l, m) in zip(amps, modes))
+    P = P + (delta / np.linalg.norm(P, axis=-1))[..., None] * P
+    V = P.reshape(-1, 3)
+    poles = []
+    for pole_theta, z in ((0.0, c), (np.pi, -c)):
+        d = sum(amp * real_sph_harm(l, m, np.array(pole_theta), np.array(0.0)) for amp, (l, m) in zip(amps, modes))
+        poles.append([0.0, 0.0, z + np.sign(z) * float(d)])
+    top, bottom = V.shape[0], V.shape[0] + 1
+    V = np.concatenate([V, np.array(poles)])
+    nr = th.size
+    T = [_grid_tris(nr - 1, n_phi, 0, wrap_v=True)]
+    j = np.arange(n_phi)
+    jn = (j + 1) % n_phi
+    T.append(np.stack([np.full(n_phi, top), j, jn], axis=1))
+    last = (nr - 1) * n_phi
+    T.append(np.stack([np.full(n_phi, bottom), last + jn, last + j], axis=1))
+    T = np.concatenate(T)
+    T = _orient_outward(V, T, centre=(0.0, 0.0, 0.0))
+    return centre_on_aabb(V), T.astype(np.uint32)
+
+
 def bounding_radius(verts) -> float:
     """Radius of the bounding sphere about the AABB centre."""
     v = np.asarray(verts, dtype=np.float64)
