@@ -177,6 +177,13 @@ typedef struct sbr_plan_info {
 
 sbr_status sbr_plan_create(sbr_scene* scene, const sbr_job* jobs, size_t n_jobs, const sbr_run_opts* opts,
                            sbr_plan** out);
+/* A plan whose jobs trace different meshes: job j traces scenes[job_scene[j]].
+ * All scenes live on one device and must outlive the plan; every job of every
+ * scene is drained by the same persistent launch.  Errors and the cancel flag
+ * are those of scenes[0]; the first-hit raster is not used.  No counterpart in
+ * the reference (one mesh per process). */
+sbr_status sbr_plan_create_multi(sbr_scene* const* scenes, size_t n_scenes, const int32_t* job_scene,
+                                 const sbr_job* jobs, size_t n_jobs, const sbr_run_opts* opts, sbr_plan** out);
 /* Launches the plan on opts->stream (or the scene stream); asynchronous. */
 sbr_status sbr_plan_execute(sbr_plan* plan);
 /* Waits for the plan and copies results to host arrays (any may be NULL). */

@@ -174,16 +174,28 @@ def _jobs_c(jobs):
 class Plan:
     """Prepared sweep (sbr_plan): frames, work items and result buffers on the GPU."""
 
-    def __init__(self, scene: Scene, jobs: Sequence[JobSpec], mode=MODE_BATCHED, precision=PREC_MIXED,
-                 stream=None, use_graph=False, ctas_per_sm=0, first_hit=None, polarization=POL_SCALAR):
+    def __init__(self, scene: Scene | Sequence[Scene], jobs: Sequence[JobSpec], mode=MODE_BATCHED,
+                 precision=PREC_MIXED, stream=None, use_graph=False, ctas_per_sm=0, first_hit=None,
+                 polarization=POL_SCALAR, job_scene: Sequence[int] | None = None):
+        """With a list of scenes, job j traces scene[job_scene[j]] (sbr_plan_create_multi)."""
         self.scene = scene
         self.jobs = list(jobs)
         self._jc = _jobs_c(self.jobs)
         o = _opts(mode, precision, polarization, stream=stream, use_graph=use_graph, ctas_per_sm=ctas_per_sm,
                   first_hit=FIRST_HIT_TRAVERSE if first_hit is None else first_hit)
         h = C.c_void_p()
-        check(lib().sbr_plan_create(scene.handle, self._jc, len(self.jobs), C.byref(o), C.byref(h)),
-              "sbr_plan_create")
+        if isinstance(scene, Scene):
+            check(lib().sbr_plan_create(scene.handle, self._jc, len(self.jobs), C.byref(o), C.byref(h)),
+                  "sbr_plan_create")
+        else:
+            scenes = list(scene)
+            js = np.ascontiguousarray(np.zeros(len(self.jobs)) if job_scene is None else job_scene, dtype=np.int32)
+            if js.size != len(self.jobs):
+                raise ValueError("job_scene needs one scene index per job")
+            hs = (C.c_void_p * len(scenes))(*[sc.handle.value for sc in scenes])
+            self._keep = (scenes, js, hs)
+            check(lib().sbr_plan_create_multi(hs, len(scenes), _p(js), self._jc, len(self.jobs), C.byref(o),
+                                              C.byref(h)), "sbr_plan_create_multi")
         self._h = h
         i = _lib.PlanInfo()
         check(lib().sbr_plan_info_get(h, C.byref(i)), "sbr_plan_info_get")

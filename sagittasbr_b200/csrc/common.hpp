@@ -105,7 +105,7 @@ struct JobConst {
     int32_t n_freqs;
     int32_t max_bounces;
     int32_t freq_base;    // index of this job's first frequency in the frequency table
-    int32_t pad;
+    int32_t scene;        // index of the job's scene in a multi-scene plan (0 otherwise)
     double inv_nx, inv_ny;
     double refl;          // reflection coefficient R
     float reflf;

@@ -94,6 +94,7 @@ void release(sbr_plan* p) {
     cudaFree(p->d_queue);
     cudaFree(p->d_zbuf);
     cudaFree(p->d_segpol);
+    cudaFree(p->d_scenes);
     if (p->ev0) cudaEventDestroy(p->ev0);
     if (p->ev1) cudaEventDestroy(p->ev1);
     delete p;
@@ -145,19 +146,22 @@ sbr_status validate_run(const sbr_scene* s, const sbr_job* jobs, size_t n_jobs, 
     return SBR_OK;
 }
 
-sbr_status build_tables(const sbr_scene* s, const sbr_job* jobs, size_t n_jobs, const sbr_run_opts& o,
-                        TableSink& sink, TableTotals& tot) {
+sbr_status build_tables(const sbr_scene* const* scenes, const int32_t* job_scene, const sbr_job* jobs,
+                        size_t n_jobs, const sbr_run_opts& o, TableSink& sink, TableTotals& tot) {
     const double c0 = 299792458.0;
-    const double* lo = s->aabb_lo;
-    const double* hi = s->aabb_hi;
-    double diag = std::sqrt((hi[0] - lo[0]) * (hi[0] - lo[0]) + (hi[1] - lo[1]) * (hi[1] - lo[1]) +
-                            (hi[2] - lo[2]) * (hi[2] - lo[2]));
     tot = TableTotals{};
     int64_t item = 0, sample = 0;
     int32_t nfreq = 0;
     for (size_t j = 0; j < n_jobs; ++j) {
         const sbr_job& J = jobs[j];
+        const int32_t si = job_scene ? job_scene[j] : 0;
+        const sbr_scene* s = scenes[si];
+        const double* lo = s->aabb_lo;
+        const double* hi = s->aabb_hi;
+        const double diag = std::sqrt((hi[0] - lo[0]) * (hi[0] - lo[0]) + (hi[1] - lo[1]) * (hi[1] - lo[1]) +
+                                      (hi[2] - lo[2]) * (hi[2] - lo[2]));
         JobConst jc{};
+        jc.scene = si;
         jc.nx = J.nx;
         jc.ny = J.ny;
         jc.n_freqs = (int32_t)J.n_freqs;
@@ -301,24 +305,40 @@ struct PlanSink : sbr::TableSink {
 
 }  // namespace
 
-extern "C" {
+namespace {
 
-sbr_status sbr_plan_create(sbr_scene* s, const sbr_job* jobs, size_t n_jobs, const sbr_run_opts* opts,
-                           sbr_plan** out) {
+// Plan over one scene (job_scene null) or several scenes on one device.
+sbr_status plan_create(sbr_scene* const* scenes, size_t n_scenes, const int32_t* job_scene, const sbr_job* jobs,
+                       size_t n_jobs, const sbr_run_opts* opts, sbr_plan** out) {
     if (!out) return fail(SBR_ERR_INVALID_ARG, "out is null");
     *out = nullptr;
+    if (!scenes || n_scenes == 0) return fail(SBR_ERR_INVALID_ARG, "no scene");
     sbr_run_opts o{};
     if (opts) o = *opts;
+    sbr_scene* s = scenes[0];
     sbr_status vs = validate_run(s, jobs, n_jobs, o);
     if (vs != SBR_OK) return vs;
+    for (size_t k = 0; k < n_scenes; ++k) {
+        if (!scenes[k]) return fail(SBR_ERR_INVALID_ARG, "null scene");
+        if (scenes[k]->device != s->device) return fail(SBR_ERR_INVALID_ARG, "scenes of one plan share a device");
+    }
+    if (job_scene)
+        for (size_t j = 0; j < n_jobs; ++j)
+            if (job_scene[j] < 0 || (size_t)job_scene[j] >= n_scenes)
+                return fail(SBR_ERR_INVALID_ARG, "job scene index out of range");
     SBR_CUDA(cudaSetDevice(s->device));
     if (o.precision == SBR_PREC_FP64) {
-        sbr_status st = ensure_fp64(s);
-        if (st != SBR_OK) return st;
+        for (size_t k = 0; k < n_scenes; ++k) {
+            sbr_status st = ensure_fp64(scenes[k]);
+            if (st != SBR_OK) return st;
+        }
     }
 
     sbr_plan* p = new sbr_plan();
     p->scene = s;
+    p->multi = job_scene != nullptr;
+    if (p->multi)
+        for (size_t k = 0; k < n_scenes; ++k) p->scene_views.push_back(scenes[k]->view());
     p->mode = o.mode;
     p->prec = o.precision;
     p->pol = o.polarization;
@@ -332,7 +352,8 @@ sbr_status sbr_plan_create(sbr_scene* s, const sbr_job* jobs, size_t n_jobs, con
 
     PlanSink sink(p);
     TableTotals tot;
-    sbr_status bs = build_tables(s, jobs, n_jobs, o, sink, tot);
+    const sbr_scene* const* cs = scenes;
+    sbr_status bs = build_tables(cs, job_scene, jobs, n_jobs, o, sink, tot);
     if (bs != SBR_OK) {
         release(p);
         return bs;
@@ -366,7 +387,7 @@ sbr_status sbr_plan_create(sbr_scene* s, const sbr_job* jobs, size_t n_jobs, con
     // first-hit rasterisation (batched FP32 / mixed): chunks of consecutive
     // segments whose per-pixel first-hit buffers fit a fixed budget
     p->raster = o.mode == SBR_MODE_BATCHED && o.precision != SBR_PREC_FP64 && o.first_hit == SBR_FIRST_HIT_RASTER &&
-                p->n_items > 0;
+                p->n_items > 0 && !p->multi;
     if (p->raster) {
         const int64_t budget = int64_t(256) << 20;  // entries (8 B each): 2 GiB
         sbr_plan::Chunk c{0, 0, 0, 0, 0};
@@ -405,6 +426,7 @@ sbr_status sbr_plan_create(sbr_scene* s, const sbr_job* jobs, size_t n_jobs, con
         (st = upload(&p->d_jobs, p->jobs, b)) != SBR_OK || (st = upload(&p->d_freqs, p->freqs, b)) != SBR_OK ||
         (st = upload(&p->d_quantum, p->quantum, b)) != SBR_OK ||
         (p->n_pol == 2 && (st = upload(&p->d_segpol, p->segpol, b)) != SBR_OK) ||
+        (p->multi && (st = upload(&p->d_scenes, p->scene_views, b)) != SBR_OK) ||
         (st = zalloc(&p->d_acc, 2 * (size_t)p->n_samples * p->n_pol * kAccReplicas, b)) != SBR_OK ||
         (st = zalloc(&p->d_acc_stats, 4 * (size_t)p->n_segs, b)) != SBR_OK ||
         (st = zalloc(&p->d_field, 2 * (size_t)p->n_samples * p->n_pol, b)) != SBR_OK ||
@@ -420,6 +442,21 @@ sbr_status sbr_plan_create(sbr_scene* s, const sbr_job* jobs, size_t n_jobs, con
     }
     *out = p;
     return SBR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+sbr_status sbr_plan_create(sbr_scene* s, const sbr_job* jobs, size_t n_jobs, const sbr_run_opts* opts,
+                           sbr_plan** out) {
+    return plan_create(&s, 1, nullptr, jobs, n_jobs, opts, out);
+}
+
+sbr_status sbr_plan_create_multi(sbr_scene* const* scenes, size_t n_scenes, const int32_t* job_scene,
+                                 const sbr_job* jobs, size_t n_jobs, const sbr_run_opts* opts, sbr_plan** out) {
+    if (!job_scene && n_jobs) return fail(SBR_ERR_INVALID_ARG, "job_scene is required");
+    return plan_create(scenes, n_scenes, job_scene, jobs, n_jobs, opts, out);
 }
 
 sbr_status sbr_plan_execute(sbr_plan* p) {

@@ -49,6 +49,9 @@ struct sbr_plan {
     int num_sms = 0;
     cudaStream_t stream = nullptr;
     sbr::SceneView scene_view{};
+    bool multi = false;                      // jobs trace different scenes (JobConst::scene)
+    std::vector<sbr::SceneView> scene_views; // multi-scene plans: one per scene
+    sbr::SceneView* d_scenes = nullptr;
 
     std::vector<sbr::Segment> segs;
     std::vector<int64_t> seg_base;     // [n_segs + 1] first item of each segment
@@ -115,8 +118,10 @@ struct TableTotals {
 // Argument checks shared by every sweep entry point.
 sbr_status validate_run(const sbr_scene* s, const sbr_job* jobs, size_t n_jobs, const sbr_run_opts& o);
 // Launcher frames, aperture clipping, work items and fixed-point units of a sweep.
-sbr_status build_tables(const sbr_scene* s, const sbr_job* jobs, size_t n_jobs, const sbr_run_opts& o,
-                        TableSink& sink, TableTotals& tot);
+// Job j is clipped against the bounds of job_scene[j] (an index into scenes) when
+// job_scene is given, else every job uses scenes[0].
+sbr_status build_tables(const sbr_scene* const* scenes, const int32_t* job_scene, const sbr_job* jobs,
+                        size_t n_jobs, const sbr_run_opts& o, TableSink& sink, TableTotals& tot);
 
 sbr_status plan_launch(sbr_plan* pl, bool records, sbr_ray_record* d_records);
 sbr_status fill_records(sbr_ray_record* d, long long n, cudaStream_t st);

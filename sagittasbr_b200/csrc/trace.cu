@@ -38,6 +38,7 @@ struct TraceParams {
     int64_t item_begin, item_end;  // items handled by this launch
     unsigned long long* queue;     // work-queue head of this launch
     const SegPol* segpol;          // [n_segs], SBR_POL_HHVV plans only
+    const SceneView* scenes;       // multi-scene plans: scene of JobConst::scene
     unsigned long long* acc;       // [n_samples][n_pol][n_rep][2] fixed-point field accumulators
     unsigned long long* acc_stats; // [n_segs * 4]
     uint32_t* err;
@@ -182,7 +183,7 @@ __device__ __forceinline__ void add_fixed(unsigned long long* acc, double v, dou
 // the warp reduces them in a fixed order and adds the total, as int64 fixed
 // point, to one of the segment's accumulator replicas.  Which lane takes which
 // ray depends only on the item, so every sum is reproducible bit for bit.
-template <int PREC, int EPI, bool REC, bool POL>
+template <int PREC, int EPI, bool REC, bool POL, bool MULTI>
 __global__ void __launch_bounds__(kCtaThreads, kMinCtasPerSm) k_trace(const TraceParams P) {
     constexpr unsigned FULL = 0xffffffffu;
     constexpr bool F64 = PREC == SBR_PREC_FP64;
@@ -210,6 +211,7 @@ __global__ void __launch_bounds__(kCtaThreads, kMinCtasPerSm) k_trace(const Trac
         const int seg = find_segment(P.seg_item_base, P.n_segs, item);
         const Segment& G = P.segs[seg];
         const JobConst J = P.jobs[G.job];
+        const SceneView S = MULTI ? P.scenes[J.scene] : P.S;
         const int kb = P.k_count > 0 ? P.k_begin : 0;
         const int K = P.k_count > 0 ? P.k_count : J.n_freqs;
         const FreqConst* F = P.freqs + J.freq_base + kb;
@@ -270,8 +272,8 @@ __global__ void __launch_bounds__(kCtaThreads, kMinCtasPerSm) k_trace(const Trac
             RayOut out;
             out.amp = 0.0f;
             if (active) {
-                done = F64 ? step_d<REC, POL>(rd, ed, P.S, J.max_bounces, err, rec)
-                           : step_f<PREC, REC, POL>(rf, ef, P.S, J.max_bounces, err, rec, P.zbuf);
+                done = F64 ? step_d<REC, POL>(rd, ed, S, J.max_bounces, err, rec)
+                           : step_f<PREC, REC, POL>(rf, ef, S, J.max_bounces, err, rec, P.zbuf);
                 ++queries;
                 if (done) {
                     const int cnt = F64 ? rd.count : rf.count;
@@ -520,27 +522,37 @@ __global__ void k_fill_records(sbr_ray_record* r, long long n) {
 // --------------------------------------------------------------------- host
 namespace {
 
-template <int PREC, int EPI, bool REC, bool POL>
+template <int PREC, int EPI, bool REC, bool POL, bool MULTI>
 const void* kernel_ptr() {
-    return reinterpret_cast<const void*>(&k_trace<PREC, EPI, REC, POL>);
+    return reinterpret_cast<const void*>(&k_trace<PREC, EPI, REC, POL, MULTI>);
 }
 
-template <int PREC, bool REC, bool POL>
+template <int PREC, bool REC, bool POL, bool MULTI = false>
 const void* pick_epi_kernel(int epi) {
     switch (epi) {
-        case EPI_LANE1: return kernel_ptr<PREC, EPI_LANE1, REC, POL>();
-        case EPI_LANE4: return kernel_ptr<PREC, EPI_LANE4, REC, POL>();
-        case EPI_T64: return kernel_ptr<PREC, EPI_T64, REC, POL>();
-        default: return kernel_ptr<PREC, EPI_T128, REC, POL>();
+        case EPI_LANE1: return kernel_ptr<PREC, EPI_LANE1, REC, POL, MULTI>();
+        case EPI_LANE4: return kernel_ptr<PREC, EPI_LANE4, REC, POL, MULTI>();
+        case EPI_T64: return kernel_ptr<PREC, EPI_T64, REC, POL, MULTI>();
+        default: return kernel_ptr<PREC, EPI_T128, REC, POL, MULTI>();
     }
 }
 
 // Trace kernel for a plan: precision, accumulator layout for `channels` (the
-// largest frequencies x polarisations of a launch), records, polarisation.
-// Record kernels come with the two general layouts only; polarised kernels in
-// MIXED and FP64 precision only (the host rejects the other combinations).
-const void* pick_kernel(int prec, int channels, bool rec, bool pol) {
+// largest frequencies x polarisations of a launch), records, polarisation, and
+// whether jobs trace different scenes.  Record kernels come with the two general
+// layouts only and one scene; polarised kernels in MIXED and FP64 precision only
+// (the host rejects the other combinations).
+const void* pick_kernel(int prec, int channels, bool rec, bool pol, bool multi = false) {
     int epi = pick_epi(channels);
+    if (multi && !rec) {
+        if (pol) return prec == SBR_PREC_FP64 ? pick_epi_kernel<SBR_PREC_FP64, false, true, true>(epi)
+                                              : pick_epi_kernel<SBR_PREC_MIXED, false, true, true>(epi);
+        switch (prec) {
+            case SBR_PREC_MIXED: return pick_epi_kernel<SBR_PREC_MIXED, false, false, true>(epi);
+            case SBR_PREC_FP32: return pick_epi_kernel<SBR_PREC_FP32, false, false, true>(epi);
+            default: return pick_epi_kernel<SBR_PREC_FP64, false, false, true>(epi);
+        }
+    }
     if (rec) {
         epi = epi <= EPI_LANE4 ? EPI_LANE4 : EPI_T128;
         switch (prec) {
@@ -585,9 +597,10 @@ sbr_status plan_launch(sbr_plan* pl, bool records, sbr_ray_record* d_records) {
     const bool pol = pl->pol == SBR_POL_HHVV && !records;
     const int npol = pol ? 2 : 1;
     const bool batched = pl->mode == SBR_MODE_BATCHED || records;
-    const void* fn = pick_kernel(pl->prec, (batched ? pl->k_max : 1) * npol, records, pol);
+    const void* fn = pick_kernel(pl->prec, (batched ? pl->k_max : 1) * npol, records, pol, pl->multi);
     TraceParams p{};
     p.segpol = pl->d_segpol;
+    p.scenes = pl->d_scenes;
     p.S = pl->scene_view;
     p.segs = pl->d_segs;
     p.seg_item_base = pl->d_seg_base;
@@ -800,7 +813,8 @@ extern "C" sbr_status sbr_run_noalloc(sbr_scene* s, const sbr_job* job, double* 
     NoallocSink sink;
     g_noalloc_host.seg_base[0] = 0;
     TableTotals tot;
-    st = build_tables(s, job, 1, o, sink, tot);
+    const sbr_scene* one[1] = {s};
+    st = build_tables(one, nullptr, job, 1, o, sink, tot);
     if (st != SBR_OK) return st;
 
     cudaStream_t stream = o.stream ? (cudaStream_t)o.stream : s->stream;

@@ -313,6 +313,64 @@ def ellipsoid_sh(axes=(2.0, 1.0, 0.5), n_theta: int = 224, n_phi: int = 448, n_m
     return centre_on_aabb(V), T.astype(np.uint32)
 
 
+def plate_cluster(n_plates: int, n: int, size: float = 0.5, spread: float = 1.0, seed: int = 0):
+    """``n_plates`` square plates (side ``size``, n x n x 2 triangles each), randomly
+    rotated and placed within a cube of side ``spread``; both faces are lit from
+    the side their normal points to."""
+    rng = np.random.default_rng(seed)
+    vs, ts, off = [], [], 0
+    for _ in range(n_plates):
+        P, T = _grid_plate(2, 0.0, -size / 2, size / 2, n)
+        q = rng.normal(size=4)
+        q /= np.linalg.norm(q)
+        w, x, y, z = q
+        Rm = np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
+                       [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
+                       [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)]])
+        vs.append(P @ Rm.T + rng.uniform(-spread / 2, spread / 2, size=3))
+        ts.append(T + off)
+        off += P.shape[0]
+    return centre_on_aabb(np.concatenate(vs)), np.concatenate(ts).astype(np.uint32)
+
+
+def uneven_batch(n_meshes: int = 64, seed: int = 5, tri_range=(1_000, 500_000)):
+    """Seeded batch of meshes of uneven cost: icospheres, trihedrals, jittered
+    SH-displaced ellipsoids and plate clusters with log-uniform triangle counts in
+    ``tri_range``; each instance has its own frequency (uniform 1-12 GHz), its own
+    azimuth sweep (90-1440 angles at a random elevation), 2-6 bounces and its own
+    aperture G = 2 R_bs with n = ceil(10 G f / c) rays per side.  Returns a list of
+    dicts (verts, tris, kind, freq, theta, phi, max_bounces, G, n)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    lo, hi = np.log(tri_range[0]), np.log(tri_range[1])
+    for i in range(n_meshes):
+        kind = ("icosphere", "trihedral", "ellipsoid", "plates")[i % 4]
+        target = float(np.exp(rng.uniform(lo, hi)))
+        size = float(rng.uniform(0.3, 1.5))
+        if kind == "icosphere":
+            level = int(np.clip(round(np.log(target / 20.0) / np.log(4.0)), 2, 7))
+            v, t = icosphere(level, size / 2)
+        elif kind == "trihedral":
+            v, t = trihedral(size, max(1, int(round(np.sqrt(target / 6.0)))))
+        elif kind == "ellipsoid":
+            nt = max(8, int(round(np.sqrt(target / 4.0))))
+            v, t = ellipsoid_sh((size, 0.6 * size, 0.35 * size), n_theta=nt, n_phi=2 * nt, sigma=0.01 * size,
+                                seed=int(rng.integers(1 << 30)))
+            v = (v + rng.normal(0.0, 1e-3 * size, v.shape)).astype(np.float32)
+        else:
+            k = int(rng.integers(3, 9))
+            n = max(1, int(round(np.sqrt(target / (2.0 * k)))))
+            v, t = plate_cluster(k, n, size / 2, size, seed=int(rng.integers(1 << 30)))
+        f = float(rng.uniform(1e9, 12e9))
+        na = int(rng.integers(90, 1441))
+        th0 = float(rng.uniform(30.0, 150.0))
+        G = 2.0 * bounding_radius(v)
+        out.append(dict(verts=v, tris=t, kind=kind, freq=f, theta=np.full(na, th0),
+                        phi=np.linspace(0.0, 360.0, na, endpoint=False), max_bounces=int(rng.integers(2, 7)),
+                        G=G, n=rays_for(f, G)))
+    return out
+
+
 def bounding_radius(verts) -> float:
     """Radius of the bounding sphere about the AABB centre."""
     v = np.asarray(verts, dtype=np.float64)

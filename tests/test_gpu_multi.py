@@ -1,0 +1,81 @@
+"""GPU checks of multi-scene plans (sbr_plan_create_multi): jobs over different
+meshes in one persistent launch give, bit for bit, the fields of separate
+single-scene runs (the fixed-point sums do not depend on which warp adds what)."""
+import numpy as np
+import pytest
+
+import sagittasbr_b200 as sbr
+from sagittasbr_b200 import meshes as M
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    import torch
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+
+
+def _batch():
+    meshes = [M.icosphere(3, 0.7), M.trihedral(0.8, 6), M.box(1.0), M.plate_cluster(4, 3, 0.4, 1.0, seed=3)]
+    jobs = [sbr.JobSpec(np.full(20, 90.0), np.linspace(0, 350, 20), [2e9, 3e9], 48, 48, 1.6, 3),
+            sbr.JobSpec(np.linspace(10, 80, 15), np.full(15, 45.0), [5e9], 64, 64, 1.5, 3),
+            sbr.JobSpec([30.0, 60.0], [10.0, 80.0], [1e9], 40, 40, 2.0, 4),
+            sbr.JobSpec(np.full(30, 60.0), np.linspace(0, 300, 30), [4e9, 6e9, 8e9], 56, 56, 2.0, 5, 0.9),
+            sbr.JobSpec([45.0, 50.0], [20.0, 25.0], [3e9], 48, 48, 1.6, 2)]
+    job_scene = [0, 1, 2, 3, 0]
+    return meshes, jobs, job_scene
+
+
+@pytest.mark.parametrize("prec,pol,mode", [(sbr.PREC_MIXED, sbr.POL_SCALAR, sbr.MODE_BATCHED),
+                                           (sbr.PREC_FP32, sbr.POL_SCALAR, sbr.MODE_BATCHED),
+                                           (sbr.PREC_FP64, sbr.POL_SCALAR, sbr.MODE_BATCHED),
+                                           (sbr.PREC_MIXED, sbr.POL_HHVV, sbr.MODE_BATCHED),
+                                           (sbr.PREC_MIXED, sbr.POL_SCALAR, sbr.MODE_PER_ANGLE)])
+def test_multi_scene_plan_matches_separate_runs(prec, pol, mode):
+    meshes, jobs, job_scene = _batch()
+    scenes = [sbr.Scene(v, t) for v, t in meshes]
+    try:
+        pl = sbr.Plan(scenes, jobs, mode=mode, precision=prec, polarization=pol, job_scene=job_scene)
+        pl.execute()
+        got = pl.results()
+        pl.close()
+        want = [sbr.run(scenes[s], j, mode=mode, precision=prec, polarization=pol) for j, s in zip(jobs, job_scene)]
+        want_f = np.concatenate([w.field for w in want])
+        # the same sums, up to the order of FP64 additions inside a warp when the plan's
+        # widest job selects another accumulator layout than a job's own run
+        np.testing.assert_allclose(got.field, want_f, rtol=1e-12, atol=1e-13 * np.abs(want_f).max())
+        assert np.array_equal(got.stats, np.concatenate([w.stats for w in want]))
+    finally:
+        for s in scenes:
+            s.close()
+
+
+def test_multi_scene_plan_graph_and_repeat():
+    meshes, jobs, job_scene = _batch()
+    scenes = [sbr.Scene(v, t) for v, t in meshes]
+    try:
+        pl = sbr.Plan(scenes, jobs, use_graph=True, job_scene=job_scene)
+        pl.execute()
+        a = pl.results()
+        pl.execute()
+        b = pl.results()
+        pl.close()
+        assert np.array_equal(a.field, b.field)
+        assert a.field.size == sum(j.n_angles * j.n_freqs for j in jobs)
+    finally:
+        for s in scenes:
+            s.close()
+
+
+def test_multi_scene_errors():
+    meshes, jobs, job_scene = _batch()
+    scenes = [sbr.Scene(v, t) for v, t in meshes[:2]]
+    try:
+        with pytest.raises(sbr.SbrError):
+            sbr.Plan(scenes, jobs[:2], job_scene=[0, 2])   # index out of range
+        with pytest.raises(ValueError):
+            sbr.Plan(scenes, jobs[:2], job_scene=[0])      # one index per job
+    finally:
+        for s in scenes:
+            s.close()
