@@ -307,6 +307,15 @@ sbr_status sbr_config_angles(const sbr_config* cfg, double* theta_deg, double* p
 /* OBJ reader (v / f records; polygons fan-triangulated).  *xyz and *tri_idx are
  * allocated with malloc; release with sbr_free. */
 sbr_status sbr_load_obj(const char* path, float** xyz, size_t* nverts, uint32_t** tri_idx, size_t* ntris);
+/* glTF 2.0 reader (.gltf with external or base64 data: buffers, binary .glb), as the
+ * reference reads it through tinygltf (src/modelLoader.cpp:286-413): every TRIANGLES
+ * primitive of every mesh in file order, FLOAT POSITION accessors, u8 / u16 / u32
+ * indices (none: vertices in order), node transforms not applied.  Outputs as
+ * sbr_load_obj. */
+sbr_status sbr_load_gltf(const char* path, float** xyz, size_t* nverts, uint32_t** tri_idx, size_t* ntris);
+/* loadModel (src/modelLoader.cpp:421-450): .obj, .gltf or .glb by extension, else
+ * SBR_ERR_UNSUPPORTED. */
+sbr_status sbr_load_model(const char* path, float** xyz, size_t* nverts, uint32_t** tri_idx, size_t* ntris);
 void sbr_free(void* p);
 /* Writes rcs_results.csv in the reference layout (rtRcsEntry.cu:298-303, sweep.cu:540-544). */
 sbr_status sbr_write_csv(const char* path, const sbr_config* cfg, const double* theta_deg, const double* phi_deg,

@@ -28,7 +28,7 @@ from ._lib import (FIRST_HIT_RASTER, FIRST_HIT_TRAVERSE, MODE_BATCHED, MODE_PER_
 
 __all__ = [
     "Scene", "JobSpec", "SweepResult", "Plan", "run", "adjoint", "trace_records", "load_config", "config_angles",
-    "load_obj", "write_csv", "run_sweep", "SbrError", "MODE_BATCHED", "MODE_PER_ANGLE", "PREC_MIXED",
+    "load_obj", "load_gltf", "load_model", "write_csv", "run_sweep", "SbrError", "MODE_BATCHED", "MODE_PER_ANGLE", "PREC_MIXED",
     "FIRST_HIT_RASTER", "FIRST_HIT_TRAVERSE",
     "PREC_FP32", "PREC_FP64", "POL_SCALAR", "POL_HHVV", "RAY_RECORD",
 ]
@@ -327,9 +327,24 @@ def config_angles(cfg: dict):
 
 
 def load_obj(path: str):
+    """OBJ mesh -> (verts float32 [V, 3], tris uint32 [T, 3]) (sbr_load_obj)."""
+    return _load("sbr_load_obj", path)
+
+
+def load_gltf(path: str):
+    """glTF 2.0 / GLB mesh -> (verts, tris) (sbr_load_gltf)."""
+    return _load("sbr_load_gltf", path)
+
+
+def load_model(path: str):
+    """loadModel: .obj, .gltf or .glb by extension (sbr_load_model)."""
+    return _load("sbr_load_model", path)
+
+
+def _load(fn: str, path: str):
     pv, pt = C.c_void_p(), C.c_void_p()
     nv, nt = C.c_size_t(), C.c_size_t()
-    check(lib().sbr_load_obj(path.encode(), C.byref(pv), C.byref(nv), C.byref(pt), C.byref(nt)), "sbr_load_obj")
+    check(getattr(lib(), fn)(path.encode(), C.byref(pv), C.byref(nv), C.byref(pt), C.byref(nt)), fn)
     try:
         v = np.ctypeslib.as_array(C.cast(pv, C.POINTER(C.c_float)), shape=(nv.value * 3,)).copy()
         t = np.ctypeslib.as_array(C.cast(pt, C.POINTER(C.c_uint32)), shape=(nt.value * 3,)).copy()

@@ -156,6 +156,8 @@ SIGNATURES = {
     "sbr_trace_records": (_I32, [_P, _P, _P, _P]),
     "sbr_run_noalloc": (_I32, [_P, _P, _P, _P, _P]),
     "sbr_adjoint": (_I32, [_P, _P, C.c_size_t, _P, _P, _P, _P]),
+    "sbr_load_gltf": (_I32, [C.c_char_p, _P, _P, _P, _P]),
+    "sbr_load_model": (_I32, [C.c_char_p, _P, _P, _P, _P]),
     "sbr_plan_create_multi": (_I32, [_P, _SZ, _P, _P, _SZ, _P, _P]),
     "sbr_config_load": (_I32, [C.c_char_p, C.c_int, _P, _P]),
     "sbr_config_angles": (_I32, [_P, _P, _P]),

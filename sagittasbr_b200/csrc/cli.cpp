@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
+#include <iomanip>
 #include <iostream>
 #include <string>
 #include <vector>
@@ -49,17 +50,14 @@ int main(int argc, char** argv) {
         std::cerr << "Error: --model is required for simulation runs.\n";
         return 1;
     }
-    if (!ends_with(model, ".obj")) {
-        if (ends_with(model, ".gltf") || ends_with(model, ".glb"))
-            std::cerr << "Error: glTF models are not supported by this build; convert '" << model << "' to OBJ.\n";
-        else
-            std::cerr << "Error: Unsupported model extension for '" << model << "'.\n";
+    if (!ends_with(model, ".obj") && !ends_with(model, ".gltf") && !ends_with(model, ".glb")) {
+        std::cerr << "Error: Unsupported model extension for '" << model << "'.\n";
         return 1;
     }
     float* xyz = nullptr;
     uint32_t* idx = nullptr;
     size_t nv = 0, nt = 0;
-    st = sbr_load_obj(model.c_str(), &xyz, &nv, &idx, &nt);
+    st = sbr_load_model(model.c_str(), &xyz, &nv, &idx, &nt);
     if (st != SBR_OK) {
         std::cerr << "Error: Failed to load model '" << model << "'.\n" << sbr_last_error() << "\n";
         return 1;
@@ -97,6 +95,22 @@ int main(int argc, char** argv) {
     if (st != SBR_OK) {
         sbr_scene_destroy(scene);
         return die("csv", st);
+    }
+    // per-angle hit statistics (src/app/sweep.cu:257-295): the hit fraction of the
+    // full nx x ny grid and the mean hit count of the rays that hit, from the
+    // counters the kernel keeps on the device (no per-ray copy to the host)
+    if (cfg.show_hit_stats) {
+        const double grid = double(cfg.nx) * double(cfg.ny);
+        for (int64_t i = 0; i < n; ++i) {
+            const double h = double(stats[4 * i + 1]), b = double(stats[4 * i + 2]);
+            std::cerr << "[R0:" << std::setw(3) << i + 1 << "/" << n << "]"
+                      << " | Theta: " << std::setw(3) << static_cast<int>(th[i]) << " deg"
+                      << " | Phi: " << std::setw(3) << static_cast<int>(ph[i]) << " deg"
+                      << " | Hit: " << std::fixed << std::setprecision(0) << 100.0 * h / grid << "%"
+                      << " | Bounces: " << std::setprecision(2) << (h > 0 ? b / h : 0.0) << "\n";
+        }
+        std::cerr.unsetf(std::ios::floatfield);
+        std::cerr << std::setprecision(6);
     }
     uint64_t rays = 0, hit = 0, bounces = 0, queries = 0;
     for (int64_t i = 0; i < n; ++i) {
