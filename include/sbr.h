@@ -87,6 +87,15 @@ sbr_status sbr_scene_info_get(const sbr_scene* scene, sbr_scene_info* out);
  * (they return SBR_ERR_CANCELLED); sbr_scene_reset_cancel clears it. */
 sbr_status sbr_scene_cancel(sbr_scene* scene);
 sbr_status sbr_scene_reset_cancel(sbr_scene* scene);
+/* New coordinates for the scene's vertices (same count, same triangles), with the
+ * BVH refitted on the GPU: triangle data and every node box are recomputed for the
+ * new positions while the tree topology is kept, instead of a full rebuild
+ * (src/scene/bvhBuilder.cpp:315-360) -- for shape optimisation, where every
+ * gradient step moves the vertices a little (traversal slows down as the
+ * deformation grows; create a new scene then).  Plans created before the update
+ * keep their launcher tables (aperture clipping, launch-plane placement): create
+ * plans after it.  No counterpart in the reference. */
+sbr_status sbr_scene_update_vertices(sbr_scene* scene, const float* xyz, size_t nverts);
 
 /* --------------------------------------------------------------------- job */
 /* One job = a list of incidence angles traced on one ray grid, with a set of

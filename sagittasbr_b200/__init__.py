@@ -28,7 +28,7 @@ from ._lib import (FIRST_HIT_RASTER, FIRST_HIT_TRAVERSE, MODE_BATCHED, MODE_PER_
 
 __all__ = [
     "Scene", "JobSpec", "SweepResult", "Plan", "run", "adjoint", "trace_records", "load_config", "config_angles",
-    "load_obj", "load_gltf", "load_model", "write_csv", "run_sweep", "SbrError", "MODE_BATCHED", "MODE_PER_ANGLE", "PREC_MIXED",
+    "load_obj", "load_gltf", "load_model", "write_csv", "run_sweep", "freq_scan", "SbrError", "MODE_BATCHED", "MODE_PER_ANGLE", "PREC_MIXED",
     "FIRST_HIT_RASTER", "FIRST_HIT_TRAVERSE",
     "PREC_FP32", "PREC_FP64", "POL_SCALAR", "POL_HHVV", "RAY_RECORD",
 ]
@@ -75,6 +75,12 @@ class Scene:
             "device_bytes": i.device_bytes, "aabb_lo": list(i.aabb_lo), "aabb_hi": list(i.aabb_hi),
             "build_ms": i.build_ms, "device": i.device, "bvh_depth": i.bvh_depth,
         }
+
+    def update_vertices(self, verts):
+        """New vertex coordinates (same count and triangles); the BVH is refitted on
+        the GPU (sbr_scene_update_vertices).  Create plans after the update."""
+        v = np.ascontiguousarray(verts, dtype=np.float32).reshape(-1, 3)
+        check(lib().sbr_scene_update_vertices(self.handle, _p(v), v.shape[0]), "sbr_scene_update_vertices")
 
     def cancel(self):
         check(lib().sbr_scene_cancel(self.handle), "sbr_scene_cancel")
@@ -372,3 +378,36 @@ def run_sweep(cfg: dict, scene: Scene, out_csv: str | None = "rcs_results.csv", 
     if out_csv:
         write_csv(out_csv, cfg, th, ph, res.sigma_m2, res.rcs_dbsm)
     return th, ph, res
+
+
+def freq_scan(cfg: dict, scene: Scene, f_start: float, f_end: float, n: int,
+              out_csv: str | None = "results_freq_scans.csv", precision=None):
+    """Frequency scan of the config's angle sweep (replaces util/run_freq_scan.sh:30-53
+    with util/plotRCS.py --scans): frequencies round(logspace(f_start, f_end, n)) on
+    the config's ray grid, traced as jobs of one plan (up to 128 frequencies share
+    each angle's trace); returns (freqs, mean sigma, sample std of sigma) over the
+    angles and appends them to `out_csv` (Frequency,Avg_RCS,Std_RCS)."""
+    th, ph = config_angles(cfg)
+    fr = np.round(np.logspace(np.log10(f_start), np.log10(f_end), n))
+    jobs = [JobSpec(th, ph, fr[k:k + 128], cfg["nx"], cfg["ny"], cfg["grid_size"], cfg["max_bounces"],
+                    cfg["reflection_const"]) for k in range(0, n, 128)]
+    res = run(scene, jobs, precision=cfg.get("precision", PREC_MIXED) if precision is None else precision)
+    blocks, off = [], 0
+    for j in jobs:  # samples are job-major, then angle, then frequency
+        m = th.size * j.n_freqs
+        blocks.append(res.sigma_m2[off:off + m].reshape(th.size, j.n_freqs))
+        off += m
+    sig = np.concatenate(blocks, axis=1)
+    mean = sig.mean(axis=0)
+    std = sig.std(axis=0, ddof=1) if th.size > 1 else np.zeros_like(mean)
+    if out_csv:
+        import csv
+        import os
+        new = not os.path.exists(out_csv) or os.path.getsize(out_csv) == 0
+        with open(out_csv, "a", newline="") as f:
+            w = csv.writer(f)
+            if new:
+                w.writerow(["Frequency", "Avg_RCS", "Std_RCS"])
+            for a, b, c in zip(fr, mean, std):
+                w.writerow([float(a), float(b), float(c)])
+    return fr, mean, std

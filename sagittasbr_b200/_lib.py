@@ -156,6 +156,7 @@ SIGNATURES = {
     "sbr_trace_records": (_I32, [_P, _P, _P, _P]),
     "sbr_run_noalloc": (_I32, [_P, _P, _P, _P, _P]),
     "sbr_adjoint": (_I32, [_P, _P, C.c_size_t, _P, _P, _P, _P]),
+    "sbr_scene_update_vertices": (_I32, [_P, _P, _SZ]),
     "sbr_load_gltf": (_I32, [C.c_char_p, _P, _P, _P, _P]),
     "sbr_load_model": (_I32, [C.c_char_p, _P, _P, _P, _P]),
     "sbr_plan_create_multi": (_I32, [_P, _SZ, _P, _P, _SZ, _P, _P]),

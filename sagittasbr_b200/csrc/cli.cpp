@@ -1,16 +1,20 @@
 // cli.cpp -- RT-RCS: drop-in for the reference executable (src/RT-RCS.cpp,
 // src/app/rtRcsEntry.cu:59-352) on top of libsbr.
 //
-//   RT-RCS --model m.obj [freq] [--config c.txt] [--model-scale s]
+//   RT-RCS --model m.obj|m.gltf|m.glb [freq] [--config c.txt] [--model-scale s]
+//          [--freq-scan F_START F_END N]
 //
-// Reads config.txt (or --config), loads the OBJ model, builds the scene, runs the
+// Reads config.txt (or --config), loads the model, builds the scene, runs the
 // whole theta x phi sweep and writes rcs_results.csv in the working directory in
 // the reference layout.  Exit status 1 on any error, with the reason on stderr.
 // The sweep runs as one batched launch on the current GPU; the optional config
 // keys `precision` (0 mixed, 1 FP32, 2 FP64) and `engine_mode` (0 batched, 1
-// per-angle) select the other paths.
+// per-angle) select the other paths.  --freq-scan runs the reference's frequency
+// scan in one process instead (results_freq_scans.csv).
 #include <algorithm>
 #include <chrono>
+#include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <iomanip>
 #include <iostream>
@@ -31,13 +35,89 @@ int die(const char* what, sbr_status st) {
     return 1;
 }
 
+// Frequency scan (replaces util/run_freq_scan.sh:30-53, which re-runs RT-RCS per
+// frequency and appends util/plotRCS.py's mean / sample standard deviation of
+// rcs_m2 over the angle sweep to results_freq_scans.csv): the N frequencies
+// round(logspace(F_START, F_END, N)) are traced as jobs of one plan on the
+// config's grid -- at most 128 frequencies per job, all sharing each angle's trace.
+int freq_scan(const sbr_config& cfg, sbr_scene* scene, double f0, double f1, int nf) {
+    int64_t n = (int64_t)std::max(0, cfg.theta_samples) * std::max(0, cfg.phi_samples);
+    std::vector<double> th(n), ph(n);
+    sbr_config_angles(&cfg, th.data(), ph.data());
+    std::vector<double> freqs(nf);
+    for (int i = 0; i < nf; ++i) {
+        const double e = nf > 1 ? std::log10(f0) + i * (std::log10(f1) - std::log10(f0)) / (nf - 1) : std::log10(f0);
+        freqs[i] = std::round(std::pow(10.0, e));
+    }
+    std::vector<sbr_job> jobs;
+    for (int k0 = 0; k0 < nf; k0 += 128)
+        jobs.push_back(sbr_job{th.data(), ph.data(), n, freqs.data() + k0, std::min(128, nf - k0), cfg.nx, cfg.ny,
+                               cfg.grid_size, cfg.max_bounces, cfg.reflection_const});
+    // samples are (job, angle, frequency of the job)
+    std::vector<double> sigma((size_t)n * nf);
+    sbr_result res{};
+    res.sigma_m2 = sigma.data();
+    sbr_run_opts ro{};
+    ro.mode = SBR_MODE_BATCHED;
+    ro.precision = cfg.precision;
+    sbr_status st = sbr_run(scene, jobs.data(), jobs.size(), &res, &ro);
+    if (st != SBR_OK) return die("frequency scan", st);
+    FILE* f = std::fopen("results_freq_scans.csv", "a");
+    if (!f) {
+        std::cerr << "Error: cannot write results_freq_scans.csv\n";
+        return 1;
+    }
+    std::fseek(f, 0, SEEK_END);
+    if (std::ftell(f) == 0) std::fprintf(f, "Frequency,Avg_RCS,Std_RCS\n");
+    size_t base = 0;
+    for (const sbr_job& J : jobs) {
+        for (int64_t k = 0; k < J.n_freqs; ++k) {
+            double s = 0.0, s2 = 0.0;
+            for (int64_t a = 0; a < n; ++a) s += sigma[base + (size_t)a * J.n_freqs + k];
+            const double mean = n > 0 ? s / double(n) : 0.0;
+            for (int64_t a = 0; a < n; ++a) {
+                const double d = sigma[base + (size_t)a * J.n_freqs + k] - mean;
+                s2 += d * d;
+            }
+            const double sd = n > 1 ? std::sqrt(s2 / double(n - 1)) : 0.0;
+            std::fprintf(f, "%.1f,%.17g,%.17g\n", J.freq_hz[k], mean, sd);
+            std::cout << "Frequency " << J.freq_hz[k] << " Hz: average RCS " << mean << " +- " << sd << " m^2\n";
+        }
+        base += (size_t)n * J.n_freqs;
+    }
+    std::fclose(f);
+    return 0;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
     std::cerr << "SagittaSBR-compatible monostatic RCS (sbr-b200)\n";
     auto t0 = std::chrono::steady_clock::now();
+    // --freq-scan F_START F_END N is this engine's own flag; the rest goes to loadConfig
+    std::vector<const char*> args;
+    double scan_f0 = 0.0, scan_f1 = 0.0;
+    int scan_n = 0;
+    for (int i = 0; i < argc; ++i) {
+        if (std::string(argv[i]) == "--freq-scan") {
+            if (i + 3 >= argc) {
+                std::cerr << "Error: --freq-scan needs F_START F_END N\n";
+                return 1;
+            }
+            scan_f0 = std::atof(argv[i + 1]);
+            scan_f1 = std::atof(argv[i + 2]);
+            scan_n = std::atoi(argv[i + 3]);
+            if (!(scan_f0 > 0) || !(scan_f1 > 0) || scan_n < 1) {
+                std::cerr << "Error: --freq-scan needs positive F_START, F_END and N >= 1\n";
+                return 1;
+            }
+            i += 3;
+            continue;
+        }
+        args.push_back(argv[i]);
+    }
     sbr_config cfg;
-    sbr_status st = sbr_config_load("config.txt", argc, (const char* const*)argv, &cfg);
+    sbr_status st = sbr_config_load("config.txt", (int)args.size(), args.data(), &cfg);
     if (st != SBR_OK) {
         std::cerr << sbr_last_error() << "\n";
         return 1;
@@ -72,6 +152,11 @@ int main(int argc, char** argv) {
     if (st != SBR_OK) return die("scene", st);
     sbr_scene_info si;
     sbr_scene_info_get(scene, &si);
+    if (scan_n > 0) {
+        const int rc = freq_scan(cfg, scene, scan_f0, scan_f1, scan_n);
+        sbr_scene_destroy(scene);
+        return rc;
+    }
 
     int64_t n = (int64_t)std::max(0, cfg.theta_samples) * std::max(0, cfg.phi_samples);
     std::vector<double> th(n), ph(n), sigma(n), dbsm(n);

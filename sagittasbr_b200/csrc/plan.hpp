@@ -34,6 +34,12 @@ struct sbr_scene {
     cudaStream_t cancel_stream = nullptr;
     int depth = 0;
     double build_ms = 0.0;
+    // refit: 4-wide node indices grouped by depth (offsets per depth), their device
+    // copy, and the per-triangle box scratch of a refit
+    std::vector<int32_t> refit_nodes;
+    std::vector<int32_t> refit_level_off;
+    int32_t* d_refit_nodes = nullptr;
+    float* d_tri_box = nullptr;
     int64_t device_bytes = 0;
 
     sbr::SceneView view() const { return sbr::SceneView{d_nodes, d_tris, d_tris64, d_tri_id}; }

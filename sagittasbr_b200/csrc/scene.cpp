@@ -48,6 +48,8 @@ void free_scene(sbr_scene* s) {
     cudaFree(s->d_tri_id);
     cudaFree(s->d_xyz);
     cudaFree(s->d_idx);
+    cudaFree(s->d_refit_nodes);
+    cudaFree(s->d_tri_box);
     cudaFree(s->d_err);
     cudaFree(s->d_cancel);
     if (s->h_flag_vals) cudaFreeHost(s->h_flag_vals);
@@ -159,6 +161,7 @@ sbr_status sbr_scene_create(const float* xyz, size_t nverts, const uint32_t* tri
     // inner child until it holds four; siblings are stored contiguously, subtrees
     // depth first.
     std::vector<GNode4> g;
+    std::vector<int32_t> level{0};  // depth of every 4-wide node (root 0), for refits
     auto leafRef = [](const BinNode& b) { return ~(b.first * 16 + b.count); };
     auto area = [](const BinNode& b) {
         float d0 = b.hi[0] - b.lo[0], d1 = b.hi[1] - b.lo[1], d2 = b.hi[2] - b.lo[2];
@@ -184,10 +187,10 @@ sbr_status sbr_scene_create(const float* xyz, size_t nverts, const uint32_t* tri
         // only opens children while need + (children - 1) stays within the walker's
         // stack capacity.
         struct Work {
-            int32_t bin, slot, need;
+            int32_t bin, slot, need, depth;
         };
         g.emplace_back();
-        std::vector<Work> work{{0, 0, 0}};
+        std::vector<Work> work{{0, 0, 0, 0}};
         while (!work.empty()) {
             const Work w = work.back();
             const int32_t b = w.bin, slot = w.slot;
@@ -213,7 +216,7 @@ sbr_status sbr_scene_create(const float* xyz, size_t nverts, const uint32_t* tri
                 const BinNode& K = tree.nodes[kids[c]];
                 if (K.left >= 0) {
                     int32_t idx = (int32_t)g.size() + (int32_t)inner.size();
-                    inner.push_back({kids[c], idx, need});
+                    inner.push_back({kids[c], idx, need, w.depth + 1});
                     fill(n, c, &K, idx);
                 } else {
                     fill(n, c, &K, leafRef(K));
@@ -221,10 +224,22 @@ sbr_status sbr_scene_create(const float* xyz, size_t nverts, const uint32_t* tri
             }
             g[slot] = n;
             g.resize(g.size() + inner.size());
+            level.resize(g.size());
+            for (const Work& q : inner) level[q.slot] = q.depth;
             for (auto it = inner.rbegin(); it != inner.rend(); ++it) work.push_back(*it);
         }
     }
     s->n_gnodes = (int64_t)g.size();
+    // nodes grouped by depth (a refit recomputes the boxes deepest level first)
+    {
+        const int32_t maxd = *std::max_element(level.begin(), level.end());
+        s->refit_level_off.assign((size_t)maxd + 2, 0);
+        for (int32_t d : level) ++s->refit_level_off[(size_t)d + 1];
+        for (size_t d = 1; d < s->refit_level_off.size(); ++d) s->refit_level_off[d] += s->refit_level_off[d - 1];
+        std::vector<int32_t> fillp(s->refit_level_off.begin(), s->refit_level_off.end() - 1);
+        s->refit_nodes.resize(g.size());
+        for (size_t k = 0; k < g.size(); ++k) s->refit_nodes[(size_t)fillp[(size_t)level[k]]++] = (int32_t)k;
+    }
 
     // leaf-ordered triangles: v0, e1, e2 in FP32 (reference FP32 arithmetic) and
     // the unit normal unit(e1 x e2) (src/cuda/rtKernels.cu:13-14,42)
