@@ -100,6 +100,15 @@ __device__ __forceinline__ float slab_nf(float nx, float fx, float ny, float fy,
     const float tf = min3f(fmaf(fx, inv.x, -oi.x), fmaf(fy, inv.y, -oi.y), fminf(fmaf(fz, inv.z, -oi.z), tMax));
     return tn <= tf * kSlabSlack ? tn : __int_as_float(0x7f800000);
 }
+// slab_nf as an entry distance and an acceptance flag: `hit` is exactly
+// slab_nf(...) <= tMax, without materialising +inf for rejected boxes.
+__device__ __forceinline__ float slab_nh(float nx, float fx, float ny, float fy, float nz, float fz, F3 inv, F3 oi,
+                                         float tMin, float tMax, bool& hit) {
+    const float tn = max3f(fmaf(nx, inv.x, -oi.x), fmaf(ny, inv.y, -oi.y), fmaxf(fmaf(nz, inv.z, -oi.z), tMin));
+    const float tf = min3f(fmaf(fx, inv.x, -oi.x), fmaf(fy, inv.y, -oi.y), fminf(fmaf(fz, inv.z, -oi.z), tMax));
+    hit = (tn <= tf * kSlabSlack) & (tn <= tMax);
+    return tn;
+}
 __device__ __forceinline__ double slab_d(double lx, double hx, double ly, double hy, double lz, double hz, D3 o,
                                          D3 inv, double tMin, double tMax) {
     double x0 = (lx - o.x) * inv.x, x1 = (hx - o.x) * inv.x;
@@ -234,18 +243,24 @@ struct Walker<false> {
                 const float4 nx = plane(np, onx), fx = plane(np, ofx), ny = plane(np, ony), fy = plane(np, ofy);
                 const float4 nz = plane(np, onz), fz = plane(np, ofz);
                 const int4 ch = __ldg(&np->child);
-                float t[4] = {slab_nf(nx.x, fx.x, ny.x, fy.x, nz.x, fz.x, inv, oi, tMin, tBest),
-                              slab_nf(nx.y, fx.y, ny.y, fy.y, nz.y, fz.y, inv, oi, tMin, tBest),
-                              slab_nf(nx.z, fx.z, ny.z, fy.z, nz.z, fz.z, inv, oi, tMin, tBest),
-                              slab_nf(nx.w, fx.w, ny.w, fy.w, nz.w, fz.w, inv, oi, tMin, tBest)};
+                bool h0, h1, h2, h3;
+                float t[4] = {slab_nh(nx.x, fx.x, ny.x, fy.x, nz.x, fz.x, inv, oi, tMin, tBest, h0),
+                              slab_nh(nx.y, fx.y, ny.y, fy.y, nz.y, fz.y, inv, oi, tMin, tBest, h1),
+                              slab_nh(nx.z, fx.z, ny.z, fy.z, nz.z, fz.z, inv, oi, tMin, tBest, h2),
+                              slab_nh(nx.w, fx.w, ny.w, fy.w, nz.w, fz.w, inv, oi, tMin, tBest, h3)};
                 int c[4] = {ch.x, ch.y, ch.z, ch.w};
                 // most visits accept exactly one child (no ordering needed); two or
-                // more are sorted and all but the nearest pushed, farthest first
-                const bool h0 = t[0] <= tBest, h1 = t[1] <= tBest, h2 = t[2] <= tBest, h3 = t[3] <= tBest;
+                // more are sorted (rejected children last) and all but the nearest
+                // pushed, farthest first
                 const int nh = int(h0) + int(h1) + int(h2) + int(h3);
                 if (nh == 1) {
                     ref = h0 ? c[0] : h1 ? c[1] : h2 ? c[2] : c[3];
                 } else if (nh > 1) {
+                    const float inf = __int_as_float(0x7f800000);
+                    t[0] = h0 ? t[0] : inf;
+                    t[1] = h1 ? t[1] : inf;
+                    t[2] = h2 ? t[2] : inf;
+                    t[3] = h3 ? t[3] : inf;
                     sort4(t, c);
                     if (t[3] <= tBest) push(c[3], t[3]);
                     if (t[2] <= tBest) push(c[2], t[2]);
