@@ -11,7 +11,8 @@ namespace sbr {
 
 // State of one ray between closest-hit queries.
 struct RayF {
-    F3 o, d, nl, dl;
+    F3 o, d, nl, dl;  // nl, dl: last hit normal and incoming direction (records, polarisation)
+    float cosl;       // n.(-d_in) at the last hit (the PO gate and obliquity)
     double L;       // FP64 path (mixed)
     float dist32;   // FP32 path (reference FP32 arithmetic)
     int count;
@@ -19,6 +20,7 @@ struct RayF {
 };
 struct RayD {
     D3 o, d, nl, dl;
+    double cosl;
     double L;
     int count;
 };
@@ -89,6 +91,7 @@ __device__ __forceinline__ void start_f(RayF& r, const Segment& G, const JobCons
     r.d = f3(G.rdf[0], G.rdf[1], G.rdf[2]);
     r.nl = f3(0, 0, 0);
     r.dl = f3(0, 0, 0);
+    r.cosl = 0.0f;
     r.dist32 = 0.0f;
     r.count = 0;
 }
@@ -119,6 +122,7 @@ __device__ __forceinline__ bool step_f(RayF& r, PolF& e, const SceneView& S, int
             e.v = pec_reflect(e.v, r.nl);
         }
     }
+    r.cosl = dot(n, f3(-r.d.x, -r.d.y, -r.d.z));
     r.nl = n;
     r.dl = r.d;
     ++r.count;
@@ -137,7 +141,7 @@ __device__ __forceinline__ RayOut finish_f(const RayF& r, const JobConst& J) {
     RayOut o;
     float Rn = 1.0f;
     for (int b = 0; b < r.count; ++b) Rn *= J.reflf;
-    const float c = dot(r.nl, f3(-r.dl.x, -r.dl.y, -r.dl.z));
+    const float c = r.cosl;
     o.cosT = c;
     o.Rn = Rn;
     o.cosD = c;
@@ -157,6 +161,7 @@ __device__ __forceinline__ void start_d(RayD& r, const Segment& G, const JobCons
     r.d = D3{-G.dir[0], -G.dir[1], -G.dir[2]};
     r.nl = D3{0, 0, 0};
     r.dl = D3{0, 0, 0};
+    r.cosl = 0.0;
     r.L = G.shift;
     r.count = 0;
 }
@@ -175,6 +180,7 @@ __device__ __forceinline__ bool step_d(RayD& r, PolD& e, const SceneView& S, int
             e.v = pec_reflect(e.v, r.nl);
         }
     }
+    r.cosl = dot(n, D3{-r.d.x, -r.d.y, -r.d.z});
     r.nl = n;
     r.dl = r.d;
     ++r.count;
@@ -191,7 +197,7 @@ __device__ __forceinline__ RayOut finish_d(const RayD& r, const JobConst& J) {
     RayOut o;
     double Rn = 1.0;
     for (int b = 0; b < r.count; ++b) Rn *= J.refl;
-    const double c = dot(r.nl, D3{-r.dl.x, -r.dl.y, -r.dl.z});
+    const double c = r.cosl;
     o.cosT = float(c);
     o.Rn = float(Rn);
     o.cosD = c;
