@@ -518,16 +518,23 @@ def main():
     adj = None
     if args.adjoint:
         cot = 8.0 * np.pi * res.field / res.field.size
-        sbr.adjoint(scene, job, cot, precision=sbr.PREC_MIXED)  # warm-up
-        a_ms = []
+        sbr.adjoint(scene, job, cot, precision=sbr.PREC_MIXED, stream=sp)  # warm-up
+        a_ms, a_dev = [], []
         for _ in range(max(1, min(args.steps, 3))):
             torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             t0 = time.perf_counter()
-            gx, gf = sbr.adjoint(scene, job, cot, precision=sbr.PREC_MIXED)
+            e0.record(stream)
+            gx, gf = sbr.adjoint(scene, job, cot, precision=sbr.PREC_MIXED, stream=sp)
+            e1.record(stream)
             a_ms.append((time.perf_counter() - t0) * 1e3)
-        adj = {"ms": float(np.mean(a_ms)), "samples_per_s": samples / (float(np.mean(a_ms)) * 1e-3),
-               "rays_per_s": info["n_rays_clipped"] / (float(np.mean(a_ms)) * 1e-3),
-               "timing": "host wall clock around sbr_adjoint (host arrays in and out)",
+            torch.cuda.synchronize()
+            a_dev.append(e0.elapsed_time(e1))
+        adj = {"ms": float(np.mean(a_dev)), "samples_per_s": samples / (float(np.mean(a_dev)) * 1e-3),
+               "rays_per_s": info["n_rays_clipped"] / (float(np.mean(a_dev)) * 1e-3),
+               "timing": "CUDA events on the launching stream around sbr_adjoint (cotangent upload, gradient "
+                         "download and the plan tables included)",
+               "wall_ms": float(np.mean(a_ms)),
                "grad_norm": float(np.linalg.norm(gx)), "lit_vertices": int((np.abs(gx).sum(axis=1) > 0).sum())}
 
     # batched mixed precision against a full-FP64 run of the same batched job

@@ -269,7 +269,7 @@ def run(scene: Scene, jobs: Sequence[JobSpec] | JobSpec, mode=MODE_BATCHED, prec
     return _result(f, s, d, st.reshape(na, 4), r.device_ms, npol)
 
 
-def adjoint(scene: Scene, jobs: Sequence[JobSpec] | JobSpec, cot, precision=PREC_MIXED):
+def adjoint(scene: Scene, jobs: Sequence[JobSpec] | JobSpec, cot, precision=PREC_MIXED, stream=None):
     """sbr_adjoint: gradient of a loss of the sweep's fields along the frozen hit paths.
 
     cot: complex [n_samples] cotangent g of each sample's field S (dLoss =
@@ -286,7 +286,7 @@ def adjoint(scene: Scene, jobs: Sequence[JobSpec] | JobSpec, cot, precision=PREC
     c2 = np.ascontiguousarray(np.stack([g.real, g.imag], axis=1).ravel())
     gx = np.zeros(3 * scene.n_vertices)
     gf = np.zeros(n)
-    o = _opts(MODE_BATCHED, precision)
+    o = _opts(MODE_BATCHED, precision, stream=stream)
     check(lib().sbr_adjoint(scene.handle, jc, len(jobs), C.byref(o), _p(c2), _p(gx), _p(gf)), "sbr_adjoint")
     return gx.reshape(-1, 3), gf
 
