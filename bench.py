@@ -268,7 +268,8 @@ def run_uneven(args, torch, sbr, dist, ws, rank, local):
     scene_s = time.perf_counter() - t0
     jobs = [sbr.JobSpec(b["theta"], b["phi"], [b["freq"]], b["n"], b["n"], b["G"], b["max_bounces"]) for b in mine]
     js = list(range(len(mine)))
-    plan = sbr.Plan(scenes, jobs, precision=sbr.PREC_MIXED, stream=sp, use_graph=True, job_scene=js)
+    plan = sbr.Plan(scenes, jobs, precision=sbr.PREC_MIXED, stream=sp, use_graph=True, job_scene=js,
+                    autotune=args.autotune)
     info = plan.info
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
@@ -297,7 +298,8 @@ def run_uneven(args, torch, sbr, dist, ws, rank, local):
     for s in range(1 + min(args.steps, 2)):
         torch.cuda.synchronize()
         a = time.perf_counter()
-        p2 = sbr.Plan(scenes, jobs, precision=sbr.PREC_MIXED, stream=sp, job_scene=js)
+        p2 = sbr.Plan(scenes, jobs, precision=sbr.PREC_MIXED, stream=sp, job_scene=js,
+                      blocks_per_item=info["blocks_per_item"], ctas_per_sm=info["ctas_per_sm"])
         p2.execute()
         r2 = p2.results()
         p2.close()
@@ -348,7 +350,8 @@ def run_uneven(args, torch, sbr, dist, ws, rank, local):
         "config": {"workload": f"uneven_64meshes_{min(tri)}-{max(tri)}tri_{int(sum(len(b['phi']) for b in batch))}samples",
                    "meshes": len(batch), "triangles_total": int(sum(tri)), "samples": int(samples),
                    "rays_launched_per_step": info["n_rays_clipped"], "mode": "batched persistent, multi-scene plan",
-                   "cuda_graph": True, "precision": "mixed",
+                   "cuda_graph": True, "precision": "mixed", "autotune": bool(args.autotune),
+                   "blocks_per_item": info["blocks_per_item"], "ctas_per_sm": info["ctas_per_sm"],
                    "l2": "flushed before every step (256 MiB write inside the timed region)",
                    "parallelism": f"{ws} GPU(s), instances split by estimated cost", "scene_build_s": scene_s},
         "mray_bounces_per_s": res.bounces * ws / (step_ms * 1e-3) / 1e6,
@@ -385,6 +388,8 @@ def main():
                     help="per-angle mode is timed on every n-th angle of the sweep")
     ap.add_argument("--first-hit", default="traverse", choices=["traverse", "raster"],
                     help="first closest hit by BVH walk (default) or by the first-hit raster")
+    ap.add_argument("--autotune", action="store_true",
+                    help="let the plan time candidate work-item sizes / grid sizes on a sample first")
     ap.add_argument("--polarization", default="scalar", choices=["scalar", "hhvv"],
                     help="the reference's scalar PO term, or HH and VV fields with E-vector tracking")
     ap.add_argument("--fp64-check", type=int, default=0,
@@ -425,8 +430,10 @@ def main():
     job = sbr.JobSpec(w["theta"], w["phi"], w["freqs"], w["nx"], w["ny"], w["G"], w["max_bounces"], w["R"])
     first_hit = sbr.FIRST_HIT_RASTER if args.first_hit == "raster" else sbr.FIRST_HIT_TRAVERSE
     pol = sbr.POL_HHVV if args.polarization == "hhvv" else sbr.POL_SCALAR
+    t_plan = time.perf_counter()
     plan = sbr.Plan(scene, [job], mode=sbr.MODE_BATCHED, precision=sbr.PREC_MIXED, stream=sp, first_hit=first_hit,
-                    polarization=pol)
+                    polarization=pol, autotune=args.autotune)
+    plan_s = time.perf_counter() - t_plan
     info = plan.info
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
@@ -472,7 +479,7 @@ def main():
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         r2 = sbr.run(scene, job, mode=sbr.MODE_BATCHED, precision=sbr.PREC_MIXED, first_hit=first_hit,
-                     polarization=pol)
+                     polarization=pol, blocks_per_item=info["blocks_per_item"])
         if s:
             e2e_ms.append((time.perf_counter() - t0) * 1e3)
     e2e_t = torch.tensor([float(np.mean(e2e_ms))], device="cuda", dtype=torch.float64)
@@ -592,7 +599,9 @@ def main():
                    "rays_launched_per_step": info["n_rays_clipped"], "max_bounces": w["max_bounces"],
                    "mode": "batched persistent", "precision": "mixed", "polarization": args.polarization,
                    "l2": "flushed before every step (256 MiB write inside the timed region)",
-                   "parallelism": f"{ws} GPU(s), independent sweeps", "scene_build_s": scene_s},
+                   "parallelism": f"{ws} GPU(s), independent sweeps", "scene_build_s": scene_s,
+                   "plan_s": plan_s, "autotune": bool(args.autotune),
+                   "blocks_per_item": info["blocks_per_item"], "ctas_per_sm": info["ctas_per_sm"]},
         "mray_bounces_per_s": bounces_step * ws / (step_ms * 1e-3) / 1e6,
         "closest_hit_queries_per_s": queries_step * ws / (step_ms * 1e-3),
         "kernel_ms": kern_ms,

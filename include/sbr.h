@@ -154,7 +154,12 @@ typedef struct sbr_run_opts {
     void* stream;             /* cudaStream_t to launch on; NULL -> the scene's own stream */
     int32_t ctas_per_sm;      /* persistent grid size per SM; 0 -> occupancy-derived */
     int32_t first_hit;        /* SBR_FIRST_HIT_* */
-    int32_t reserved[6];
+    int32_t blocks_per_item;  /* 8x4-ray blocks per work item; 0 -> automatic (batched: blocks / 1024
+                                 clamped to 1..8 per angle, per-angle mode: 1) */
+    int32_t autotune;         /* 1: sbr_plan_create times candidate (blocks_per_item, ctas_per_sm)
+                                 settings on a sample of the plan's angles and keeps the fastest
+                                 (batched mode; adds about 20 short launches to plan creation) */
+    int32_t reserved[4];
 } sbr_run_opts;
 
 /* Results for every (job, angle, frequency[, polarization]) in job order, then
@@ -182,6 +187,8 @@ typedef struct sbr_plan_info {
     int64_t device_bytes;
     int64_t h2d_bytes;        /* bytes sbr_plan_create copies host -> device */
     int64_t d2h_bytes;        /* bytes sbr_plan_results copies device -> host (field, stats, error word) */
+    int32_t blocks_per_item;  /* the plan's setting (0: automatic per angle) */
+    int32_t ctas_per_sm;      /* persistent CTAs per SM of the trace launches */
 } sbr_plan_info;
 
 sbr_status sbr_plan_create(sbr_scene* scene, const sbr_job* jobs, size_t n_jobs, const sbr_run_opts* opts,

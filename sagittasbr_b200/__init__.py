@@ -160,13 +160,15 @@ class SweepResult:
 
 
 def _opts(mode, precision, polarization=POL_SCALAR, stream=None, use_graph=False, ctas_per_sm=0,
-          first_hit=FIRST_HIT_TRAVERSE):
+          first_hit=FIRST_HIT_TRAVERSE, blocks_per_item=0, autotune=False):
     o = _lib.RunOpts()
     o.mode, o.precision, o.polarization = int(mode), int(precision), int(polarization)
     o.use_graph = 1 if use_graph else 0
     o.stream = stream
     o.ctas_per_sm = int(ctas_per_sm)
     o.first_hit = int(first_hit)
+    o.blocks_per_item = int(blocks_per_item)
+    o.autotune = 1 if autotune else 0
     return o
 
 
@@ -182,13 +184,17 @@ class Plan:
 
     def __init__(self, scene: Scene | Sequence[Scene], jobs: Sequence[JobSpec], mode=MODE_BATCHED,
                  precision=PREC_MIXED, stream=None, use_graph=False, ctas_per_sm=0, first_hit=None,
-                 polarization=POL_SCALAR, job_scene: Sequence[int] | None = None):
-        """With a list of scenes, job j traces scene[job_scene[j]] (sbr_plan_create_multi)."""
+                 polarization=POL_SCALAR, job_scene: Sequence[int] | None = None, blocks_per_item=0,
+                 autotune=False):
+        """With a list of scenes, job j traces scene[job_scene[j]] (sbr_plan_create_multi).
+        autotune=True times candidate (blocks_per_item, ctas_per_sm) settings on a sample of
+        the angles first and keeps the fastest (batched mode); info reports the choice."""
         self.scene = scene
         self.jobs = list(jobs)
         self._jc = _jobs_c(self.jobs)
         o = _opts(mode, precision, polarization, stream=stream, use_graph=use_graph, ctas_per_sm=ctas_per_sm,
-                  first_hit=FIRST_HIT_TRAVERSE if first_hit is None else first_hit)
+                  first_hit=FIRST_HIT_TRAVERSE if first_hit is None else first_hit,
+                  blocks_per_item=blocks_per_item, autotune=autotune)
         h = C.c_void_p()
         if isinstance(scene, Scene):
             check(lib().sbr_plan_create(scene.handle, self._jc, len(self.jobs), C.byref(o), C.byref(h)),
@@ -248,7 +254,7 @@ def _result(f, s, d, st, ms, npol):
 
 
 def run(scene: Scene, jobs: Sequence[JobSpec] | JobSpec, mode=MODE_BATCHED, precision=PREC_MIXED,
-        stream=None, first_hit=None, polarization=POL_SCALAR) -> SweepResult:
+        stream=None, first_hit=None, polarization=POL_SCALAR, blocks_per_item=0) -> SweepResult:
     """One call through sbr_run: host arrays in, host arrays out.  With
     polarization=POL_HHVV the fields, sigma and dBsm carry a trailing (HH, VV) axis."""
     if isinstance(jobs, JobSpec):
@@ -264,7 +270,7 @@ def run(scene: Scene, jobs: Sequence[JobSpec] | JobSpec, mode=MODE_BATCHED, prec
     r = _lib.Result()
     r.field, r.sigma_m2, r.rcs_dbsm, r.stats = f.ctypes.data, s.ctypes.data, d.ctypes.data, st.ctypes.data
     o = _opts(mode, precision, polarization, stream=stream,
-              first_hit=FIRST_HIT_TRAVERSE if first_hit is None else first_hit)
+              first_hit=FIRST_HIT_TRAVERSE if first_hit is None else first_hit, blocks_per_item=blocks_per_item)
     check(lib().sbr_run(scene.handle, jc, len(jobs), C.byref(r), C.byref(o)), "sbr_run")
     return _result(f, s, d, st.reshape(na, 4), r.device_ms, npol)
 

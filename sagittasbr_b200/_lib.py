@@ -71,7 +71,9 @@ class RunOpts(C.Structure):
         ("stream", C.c_void_p),
         ("ctas_per_sm", C.c_int32),
         ("first_hit", C.c_int32),
-        ("reserved", C.c_int32 * 6),
+        ("blocks_per_item", C.c_int32),
+        ("autotune", C.c_int32),
+        ("reserved", C.c_int32 * 4),
     ]
 
 
@@ -97,6 +99,8 @@ class PlanInfo(C.Structure):
         ("device_bytes", C.c_int64),
         ("h2d_bytes", C.c_int64),
         ("d2h_bytes", C.c_int64),
+        ("blocks_per_item", C.c_int32),
+        ("ctas_per_sm", C.c_int32),
     ]
 
 

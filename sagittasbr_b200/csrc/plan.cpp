@@ -267,6 +267,7 @@ sbr_status build_tables(const sbr_scene* const* scenes, const int32_t* job_scene
             // segment is small; one block per item in per-angle mode, where a single
             // segment must spread over the whole GPU
             int bpi = o.mode == SBR_MODE_BATCHED ? std::max(1, std::min(8, g.blocks / 1024)) : 1;
+            if (o.blocks_per_item > 0) bpi = std::min(o.blocks_per_item, 1024);
             g.blocks_per_item = bpi;
             g.item_base = item;
             g.sample_base = sample;
@@ -307,6 +308,62 @@ struct PlanSink : sbr::TableSink {
 
 namespace {
 
+sbr_status plan_create(sbr_scene* const* scenes, size_t n_scenes, const int32_t* job_scene, const sbr_job* jobs,
+                       size_t n_jobs, const sbr_run_opts* opts, sbr_plan** out);
+
+// Autotuner of batched plans: every candidate (blocks per work item, persistent
+// CTAs per SM) -- the automatic setting among them -- runs a sample of the plan
+// (up to 128 angles spread evenly over the jobs' angle lists) twice, the second
+// run timed on the device, and the fastest setting is written into `o`.
+sbr_status autotune(sbr_scene* const* scenes, size_t n_scenes, const int32_t* job_scene, const sbr_job* jobs,
+                    size_t n_jobs, sbr_run_opts& o) {
+    const int64_t per_job = std::max<int64_t>(2, 128 / (int64_t)std::max<size_t>(1, n_jobs));
+    std::vector<std::vector<double>> th(n_jobs), ph(n_jobs);
+    std::vector<sbr_job> sj(jobs, jobs + n_jobs);
+    for (size_t j = 0; j < n_jobs; ++j) {
+        const int64_t na = jobs[j].n_angles, m = std::min(na, per_job);
+        for (int64_t q = 0; q < m; ++q) {
+            const int64_t a = m > 1 ? (q * (na - 1)) / (m - 1) : 0;
+            th[j].push_back(jobs[j].theta_deg[a]);
+            ph[j].push_back(jobs[j].phi_deg[a]);
+        }
+        sj[j].theta_deg = th[j].data();
+        sj[j].phi_deg = ph[j].data();
+        sj[j].n_angles = m;
+    }
+    const int bpis[] = {0, 1, 2, 4, 8, 16};
+    const int ctas[] = {0, 6};
+    double best = INFINITY;
+    int best_bpi = 0, best_ctas = 0;
+    for (int c : ctas) {
+        for (int b : bpis) {
+            sbr_run_opts t = o;
+            t.autotune = 0;
+            t.use_graph = 0;
+            t.blocks_per_item = b;
+            t.ctas_per_sm = c;
+            sbr_plan* pl = nullptr;
+            sbr_status st = plan_create(scenes, n_scenes, job_scene, sj.data(), n_jobs, &t, &pl);
+            if (st != SBR_OK) return st;
+            sbr_result r{};
+            for (int rep = 0; rep < 2 && st == SBR_OK; ++rep) {
+                st = sbr_plan_execute(pl);
+                if (st == SBR_OK) st = sbr_plan_results(pl, &r);
+            }
+            sbr_plan_destroy(pl);
+            if (st != SBR_OK) return st;
+            if (r.device_ms < best) {
+                best = r.device_ms;
+                best_bpi = b;
+                best_ctas = c;
+            }
+        }
+    }
+    o.blocks_per_item = best_bpi;
+    o.ctas_per_sm = best_ctas;
+    return SBR_OK;
+}
+
 // Plan over one scene (job_scene null) or several scenes on one device.
 sbr_status plan_create(sbr_scene* const* scenes, size_t n_scenes, const int32_t* job_scene, const sbr_job* jobs,
                        size_t n_jobs, const sbr_run_opts* opts, sbr_plan** out) {
@@ -318,6 +375,7 @@ sbr_status plan_create(sbr_scene* const* scenes, size_t n_scenes, const int32_t*
     sbr_scene* s = scenes[0];
     sbr_status vs = validate_run(s, jobs, n_jobs, o);
     if (vs != SBR_OK) return vs;
+    if (o.blocks_per_item < 0 || o.ctas_per_sm < 0) return fail(SBR_ERR_INVALID_ARG, "negative tuning option");
     for (size_t k = 0; k < n_scenes; ++k) {
         if (!scenes[k]) return fail(SBR_ERR_INVALID_ARG, "null scene");
         if (scenes[k]->device != s->device) return fail(SBR_ERR_INVALID_ARG, "scenes of one plan share a device");
@@ -334,8 +392,14 @@ sbr_status plan_create(sbr_scene* const* scenes, size_t n_scenes, const int32_t*
         }
     }
 
+    if (o.autotune && o.mode == SBR_MODE_BATCHED && n_jobs > 0) {
+        sbr_status st = autotune(scenes, n_scenes, job_scene, jobs, n_jobs, o);
+        if (st != SBR_OK) return st;
+    }
+
     sbr_plan* p = new sbr_plan();
     p->scene = s;
+    p->blocks_per_item = o.blocks_per_item;
     p->multi = job_scene != nullptr;
     if (p->multi)
         for (size_t k = 0; k < n_scenes; ++k) p->scene_views.push_back(scenes[k]->view());
@@ -529,6 +593,8 @@ sbr_status sbr_plan_info_get(const sbr_plan* p, sbr_plan_info* out) {
     out->n_rays_clipped = p->n_rays_clipped;
     out->n_rays_grid = p->n_rays_grid;
     out->n_pol = p->n_pol;
+    out->blocks_per_item = p->blocks_per_item;
+    out->ctas_per_sm = p->ctas_per_sm;
     int64_t launches = 1;
     if (p->mode == SBR_MODE_BATCHED && p->raster) {
         for (const auto& ch : p->chunks) launches += 1 + (ch.item_end > ch.item_begin ? 1 : 0);

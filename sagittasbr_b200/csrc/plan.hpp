@@ -52,6 +52,7 @@ struct sbr_plan {
     int pol = SBR_POL_SCALAR;
     int use_graph = 0;
     int ctas_per_sm = 0;
+    int blocks_per_item = 0;
     int num_sms = 0;
     cudaStream_t stream = nullptr;
     sbr::SceneView scene_view{};

@@ -79,3 +79,25 @@ def test_multi_scene_errors():
     finally:
         for s in scenes:
             s.close()
+
+
+def test_blocks_per_item_and_autotune_keep_the_fields():
+    """Work-item size and persistent grid change only how the rays are dealt out:
+    fields agree to the FP64 summation order, stats exactly; the autotuner picks
+    one of its candidates and reports it."""
+    v, t = M.trihedral(1.0, 10)
+    job = sbr.JobSpec(np.linspace(20, 70, 12), np.linspace(10, 80, 12), [5e9, 7e9], 96, 96, 1.8, 3)
+    with sbr.Scene(v, t) as sc:
+        base = sbr.run(sc, job)
+        for kw in ({"blocks_per_item": 1}, {"blocks_per_item": 16, "ctas_per_sm": 6}, {"autotune": True}):
+            pl = sbr.Plan(sc, [job], **kw)
+            pl.execute()
+            r = pl.results()
+            info = pl.info
+            pl.close()
+            np.testing.assert_allclose(r.field, base.field, rtol=1e-12, atol=1e-13 * np.abs(base.field).max())
+            assert np.array_equal(r.stats, base.stats)
+            if kw.get("autotune"):
+                assert info["blocks_per_item"] in (0, 1, 2, 4, 8, 16) and info["ctas_per_sm"] in (0, 6)
+            else:
+                assert info["blocks_per_item"] == kw["blocks_per_item"]
