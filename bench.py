@@ -27,6 +27,9 @@ All meshes are synthetic and seeded; no dataset is involved.
 `per_angle`  the reference's loop structure: one trace + PO launch per (angle,
              frequency), each frequency on its own grid n_f = ceil(10 G f / c), FP32
              arithmetic (the baseline of the >= 10x target), on a subset of angles.
+`reference_gpu` the reference's OWN GPU sweep (runSweep with its RT and PO kernels),
+             compiled for sm_100a from its sources (baseline/Makefile), timed on the same
+             GPU on a grid of angles; its USE_DOUBLE build is compared with the engine.
 `fp64_check` batched mixed precision against a full-FP64 run of the same batched job.
 `roofline`   dominant kernel (k_trace): algorithmic FP32 work per closest-hit query
              on the reference SAH tree, 27 V_box + 57 V_tri FLOP, V_box / V_tri counted
@@ -95,6 +98,62 @@ def workload(name: str, rank: int = 0):
     label = f"{name}_{t.shape[0]}tri_{len(freqs)}f_{min(freqs)/1e9:g}-{max(freqs)/1e9:g}GHz_{n}x{n}_{mb}b_{th.size}ang"
     return dict(verts=v, tris=t, theta=th, phi=ph, freqs=freqs, grid=grid, nx=n, ny=n, G=G, max_bounces=mb,
                 R=1.0, name=label, workload=name)
+
+
+# (theta, phi) grids, as (start, end, samples), on which the reference's own GPU build
+# is run: the timed sample (its own ray grid per frequency) and the FP64-build sample
+# (the batched grid for every frequency) compared with the engine
+REF_GPU_SAMPLES = {
+    "trihedral": (((0.0, 90.0, 91), (0.0, 88.0, 12)), ((0.0, 90.0, 8), (0.0, 90.0, 8))),
+    "sphere": (((90.0, 90.0, 1), (0.0, 352.0, 45)), ((90.0, 90.0, 1), (0.0, 350.0, 36))),
+    "aircraft": (((90.0, 90.0, 1), (0.0, 360.0, 91)), ((90.0, 90.0, 1), (0.0, 315.0, 8))),
+    "aircraft-dev": (((90.0, 90.0, 1), (0.0, 360.0, 73)), ((90.0, 90.0, 1), (0.0, 315.0, 8))),
+    "ellipsoid": (((90.0, 90.0, 1), (-30.0, 30.0, 121)), ((90.0, 90.0, 1), (-30.0, 30.0, 25))),
+}
+
+
+def ref_gpu_leg(w, sbr, scene, value):
+    """The reference's own GPU sweep (runSweep, FP32 build) timed on the same GPU, and
+    its USE_DOUBLE build compared with the engine's batched mixed-precision result."""
+    from baseline import ref_gpu
+    if not ref_gpu.available(32):
+        return {"unavailable": "baseline/_ref/libsbrrefgpu32.so not built (make -C baseline)"}
+    (th, ph), (th64, ph64) = REF_GPU_SAMPLES[w["workload"]]
+    freqs = w["freqs"]
+    nf = len(freqs)
+    r = ref_gpu.sweep(w["verts"], w["tris"], freqs, [w["grid"][f] for f in freqs], w["G"], w["max_bounces"],
+                      w["R"], th, ph, bits=32)
+    n = r["sigma"].size
+    wall, kern = float(r["wall_s"].sum()), float(r["kernel_ms"].sum())
+    out = {"value": n / wall, "unit": "samples/s", "samples": n, "angles": th[2] * ph[2], "freqs": nf,
+           "theta": list(th), "phi": list(ph), "wall_s": wall,
+           "kernel_only_value": n / (kern * 1e-3) if kern > 0 else None,
+           "batched_speedup": value / (n / wall),
+           "grids": "own grid per frequency, n_f = ceil(10 G f / c)",
+           "what": "the reference's runSweep (launchRaysMultiBounce + integratePoMultiBounce per angle and "
+                   "frequency, float atomics), FP32 build (--use_fast_math) compiled for sm_100a, one rank; "
+                   "value = samples / wall time of its runSweep calls"}
+    if ref_gpu.available(64):
+        r64 = ref_gpu.sweep(w["verts"], w["tris"], freqs, [w["nx"]] * nf, w["G"], w["max_bounces"], w["R"],
+                            th64, ph64, bits=64)
+        job = sbr.JobSpec(r64["theta"], r64["phi"], freqs, w["nx"], w["ny"], w["G"], w["max_bounces"], w["R"])
+        ours = sbr.run(scene, job, mode=sbr.MODE_BATCHED, precision=sbr.PREC_MIXED)
+        ours64 = sbr.run(scene, job, mode=sbr.MODE_BATCHED, precision=sbr.PREC_FP64)
+        ref_s = r64["sigma"].T  # [angle, freq], the engine's order
+        db_ref = 10 * np.log10(np.maximum(ref_s, 1e-10))
+        db = 10 * np.log10(np.maximum(ours.sigma_m2.reshape(ref_s.shape), 1e-10))
+        db64 = 10 * np.log10(np.maximum(ours64.sigma_m2.reshape(ref_s.shape), 1e-10))
+        lit = db_ref > db_ref.max(axis=0)[None, :] - 30.0
+        d, d64 = np.abs(db - db_ref), np.abs(db64 - db_ref)
+        out["fp64_build_vs_engine"] = {
+            "samples": int(ref_s.size), "theta": list(th64), "phi": list(ph64), "grid": w["nx"],
+            "mixed_max_abs_ddb": float(d.max()), "mixed_frac_within_0.1dB": float((d <= 0.1).mean()),
+            "mixed_max_abs_ddb_within_30dB_of_peak": float(d[lit].max()),
+            "fp64_max_abs_ddb": float(d64.max()),
+            "fp64_max_rel_sigma_diff_within_30dB_of_peak": float(
+                (np.abs(ours64.sigma_m2.reshape(ref_s.shape) - ref_s) / ref_s)[lit].max()),
+            "ref_fp64_wall_s": float(r64["wall_s"].sum())}
+    return out
 
 
 def dist_env():
@@ -392,6 +451,8 @@ def main():
                     help="let the plan time candidate work-item sizes / grid sizes on a sample first")
     ap.add_argument("--polarization", default="scalar", choices=["scalar", "hhvv"],
                     help="the reference's scalar PO term, or HH and VV fields with E-vector tracking")
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="skip the reference's own GPU build (baseline/_ref) on the same GPU")
     ap.add_argument("--fp64-check", type=int, default=0,
                     help="compare with a full-FP64 run of the batched job on this many angles")
     args = ap.parse_args()
@@ -571,6 +632,9 @@ def main():
         return 0
 
     peak = fp32_peak_tflops(torch)
+    refg = None
+    if not args.no_ref_gpu and ws == 1 and args.angles == 0 and args.workload in REF_GPU_SAMPLES:
+        refg = ref_gpu_leg(w, sbr, scene, value)
     cpu = None
     vbox = vtri = None
     if not args.no_cpu and ws == 1:
@@ -606,6 +670,7 @@ def main():
         "closest_hit_queries_per_s": queries_step * ws / (step_ms * 1e-3),
         "kernel_ms": kern_ms,
         "per_angle": per_angle,
+        "reference_gpu": refg,
         "fp64_check": fp64,
         "adjoint": adj,
         "e2e": {"value": e2e_value, "unit": "samples/s", "h2d_bytes_per_step": info["h2d_bytes"],
