@@ -311,6 +311,9 @@ typedef struct sbr_config {
     /* optional keys of this engine (absent from reference configs, which keep the defaults) */
     int32_t precision;        /* key "precision": SBR_PREC_* (default SBR_PREC_MIXED) */
     int32_t mode;             /* key "engine_mode": SBR_MODE_* (default SBR_MODE_BATCHED) */
+    int32_t csv_digits;       /* key "csv_digits" or flag --full-precision (17): significant digits
+                                 of the rcs_results.csv rows; 0 -> 6, the reference's default
+                                 ostream formatting */
 } sbr_config;
 
 /* loadConfig (src/app/config.cpp:39-155): reads `default_path` (or --config),
@@ -333,7 +336,9 @@ sbr_status sbr_load_gltf(const char* path, float** xyz, size_t* nverts, uint32_t
  * SBR_ERR_UNSUPPORTED. */
 sbr_status sbr_load_model(const char* path, float** xyz, size_t* nverts, uint32_t** tri_idx, size_t* ntris);
 void sbr_free(void* p);
-/* Writes rcs_results.csv in the reference layout (rtRcsEntry.cu:298-303, sweep.cu:540-544). */
+/* Writes rcs_results.csv in the reference layout (rtRcsEntry.cu:298-303, sweep.cu:540-544);
+ * rows with cfg->csv_digits significant digits (0: 6, as the reference; 17 round-trips a
+ * double).  The header lines keep the reference's formatting. */
 sbr_status sbr_write_csv(const char* path, const sbr_config* cfg, const double* theta_deg, const double* phi_deg,
                          const double* sigma_m2, const double* rcs_dbsm, int64_t n);
 

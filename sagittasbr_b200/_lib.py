@@ -127,6 +127,7 @@ class Config(C.Structure):
         ("freq_source", C.c_int32),
         ("precision", C.c_int32),
         ("mode", C.c_int32),
+        ("csv_digits", C.c_int32),
     ]
 
 

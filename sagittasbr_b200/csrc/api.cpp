@@ -7,6 +7,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <iomanip>
 #include <iostream>
 #include <map>
 #include <sstream>
@@ -138,6 +139,7 @@ sbr_status sbr_config_load(const char* default_path, int argc, const char* const
     c.mode = SBR_MODE_BATCHED;
     if (has("precision")) c.precision = (int32_t)kv["precision"];
     if (has("engine_mode")) c.mode = (int32_t)kv["engine_mode"];
+    if (has("csv_digits")) c.csv_digits = (int32_t)kv["csv_digits"];
 
     bool freqCli = false;
     for (int i = 1; i < argc; ++i) {
@@ -154,6 +156,10 @@ sbr_status sbr_config_load(const char* default_path, int argc, const char* const
         }
         if (a == "--config") {
             ++i;
+            continue;
+        }
+        if (a == "--full-precision") {
+            c.csv_digits = 17;
             continue;
         }
         if (!a.empty() && a[0] != '-') {
@@ -276,12 +282,14 @@ sbr_status sbr_load_obj(const char* path, float** xyz, size_t* nverts, uint32_t*
 sbr_status sbr_write_csv(const char* path, const sbr_config* c, const double* theta, const double* phi,
                          const double* sigma, const double* dbsm, int64_t n) {
     if (!path || !c || (n > 0 && (!theta || !phi || !sigma || !dbsm))) return fail(SBR_ERR_INVALID_ARG, "null argument");
+    if (c->csv_digits < 0 || c->csv_digits > 17) return fail(SBR_ERR_INVALID_ARG, "csv_digits must be 0..17");
     std::ofstream f(path);
     if (!f.is_open()) return fail(SBR_ERR_IO, std::string("cannot write ") + path);
     // default ostream formatting (6 significant digits), as the reference's
     f << "# Frequency: " << c->freq << "\n# Grid: " << c->nx << "x" << c->ny << "\n";
     f << "# GridSize: " << c->grid_size << "\n# ThetaSamples: " << c->theta_samples << "\n";
     f << "# PhiSamples: " << c->phi_samples << "\n" << "theta,phi,rcs_m2,rcs_dbsm\n";
+    if (c->csv_digits > 0) f << std::setprecision(c->csv_digits);
     for (int64_t i = 0; i < n; ++i) f << theta[i] << "," << phi[i] << "," << sigma[i] << "," << dbsm[i] << "\n";
     if (!f.good()) return fail(SBR_ERR_IO, std::string("write failed: ") + path);
     return SBR_OK;

@@ -159,6 +159,26 @@ def test_csv_layout(tmp_path):
         "theta,phi,rcs_m2,rcs_dbsm", "90,0,3.15273,4.98687", "90,6.2069,3.1511,4.98463"]
 
 
+def test_csv_full_precision_round_trips(tmp_path):
+    """csv_digits 17 (config key or --full-precision) writes rows that read back to the
+    same doubles; the header keeps the reference's formatting."""
+    (tmp_path / "config.txt").write_text("csv_digits 17\n")
+    cfg = sbr.load_config(str(tmp_path / "config.txt"), [])
+    assert cfg["csv_digits"] == 17
+    assert sbr.load_config(str(tmp_path / "none"), ["--full-precision"])["csv_digits"] == 17
+    cfg.update(freq=1e10, nx=10000, ny=10000, grid_size=2.5, theta_samples=1, phi_samples=2)
+    vals = np.array([[90.0, 0.1 + 0.2, np.pi, 10 * np.log10(np.pi)], [90.0, 6.2068965517241379, 1e-10 / 3, -100.0]])
+    out = tmp_path / "rcs_results.csv"
+    sbr.write_csv(str(out), cfg, vals[:, 0], vals[:, 1], vals[:, 2], vals[:, 3])
+    lines = out.read_text().splitlines()
+    assert lines[0] == "# Frequency: 1e+10"
+    back = np.array([[float(x) for x in ln.split(",")] for ln in lines[6:]])
+    assert np.array_equal(back, vals)
+    cfg["csv_digits"] = 18
+    with pytest.raises(sbr.SbrError):
+        sbr.write_csv(str(out), cfg, vals[:, 0], vals[:, 1], vals[:, 2], vals[:, 3])
+
+
 def test_scene_requires_gpu_or_reports_cleanly():
     """Without a device the library reports SBR_ERR_NO_DEVICE (never a CPU fallback);
     invalid meshes are rejected before any device work."""
