@@ -109,6 +109,58 @@ __device__ __forceinline__ float slab_nh(float nx, float fx, float ny, float fy,
     hit = (tn <= tf * kSlabSlack) & (tn <= tMax);
     return tn;
 }
+// Two-wide FP32 (sm_100 `fma.rn.f32x2`): both halves rounded exactly as fmaf, so
+// a pair of slab planes costs one instruction and equals the scalar form bit for bit.
+__device__ __forceinline__ unsigned long long pack2(float a, float b) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ void unpack2(unsigned long long v, float& a, float& b) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+__device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigned long long b,
+                                                   unsigned long long c) {
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+// Ray constants of slab4_nh: every axis' reciprocal direction and -o * inv, each
+// duplicated into both halves of a pair.
+struct Slab2 {
+    unsigned long long ix, iy, iz, ox, oy, oz;
+};
+__device__ __forceinline__ Slab2 slab2(F3 inv, F3 oi) {
+    return {pack2(inv.x, inv.x), pack2(inv.y, inv.y), pack2(inv.z, inv.z),
+            pack2(-oi.x, -oi.x), pack2(-oi.y, -oi.y), pack2(-oi.z, -oi.z)};
+}
+// slab_nh for the four children of a node at once (planes already ordered by the
+// ray's direction signs): the 24 plane distances as 12 two-wide FMAs, children
+// (0, 1) and (2, 3) paired.  Same entry distances and flags as four slab_nh calls.
+__device__ __forceinline__ void slab4_nh(const float4& nx, const float4& fx, const float4& ny, const float4& fy,
+                                         const float4& nz, const float4& fz, const Slab2& R, float tMin, float tMax,
+                                         float (&t)[4], bool (&h)[4]) {
+    float xn[4], xf[4], yn[4], yf[4], zn[4], zf[4];
+    unpack2(fma2(pack2(nx.x, nx.y), R.ix, R.ox), xn[0], xn[1]);
+    unpack2(fma2(pack2(nx.z, nx.w), R.ix, R.ox), xn[2], xn[3]);
+    unpack2(fma2(pack2(fx.x, fx.y), R.ix, R.ox), xf[0], xf[1]);
+    unpack2(fma2(pack2(fx.z, fx.w), R.ix, R.ox), xf[2], xf[3]);
+    unpack2(fma2(pack2(ny.x, ny.y), R.iy, R.oy), yn[0], yn[1]);
+    unpack2(fma2(pack2(ny.z, ny.w), R.iy, R.oy), yn[2], yn[3]);
+    unpack2(fma2(pack2(fy.x, fy.y), R.iy, R.oy), yf[0], yf[1]);
+    unpack2(fma2(pack2(fy.z, fy.w), R.iy, R.oy), yf[2], yf[3]);
+    unpack2(fma2(pack2(nz.x, nz.y), R.iz, R.oz), zn[0], zn[1]);
+    unpack2(fma2(pack2(nz.z, nz.w), R.iz, R.oz), zn[2], zn[3]);
+    unpack2(fma2(pack2(fz.x, fz.y), R.iz, R.oz), zf[0], zf[1]);
+    unpack2(fma2(pack2(fz.z, fz.w), R.iz, R.oz), zf[2], zf[3]);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float tn = max3f(xn[k], yn[k], fmaxf(zn[k], tMin));
+        const float tf = min3f(xf[k], yf[k], fminf(zf[k], tMax));
+        h[k] = (tn <= tf * kSlabSlack) & (tn <= tMax);
+        t[k] = tn;
+    }
+}
 __device__ __forceinline__ double slab_d(double lx, double hx, double ly, double hy, double lz, double hz, D3 o,
                                          D3 inv, double tMin, double tMax) {
     double x0 = (lx - o.x) * inv.x, x1 = (hx - o.x) * inv.x;
@@ -212,6 +264,7 @@ struct Walker<false> {
                                                   uint32_t& err) {
         const F3 inv{slab_inv(d.x), slab_inv(d.y), slab_inv(d.z)};
         const F3 oi{o.x * inv.x, o.y * inv.y, o.z * inv.z};
+        const Slab2 R2 = slab2(inv, oi);
         // byte offsets of each axis' near and far planes within a GNode4 (lo planes
         // at 0 / 32 / 64, hi planes 16 bytes after them): the ray's direction signs
         // decide which plane enters a slab, so the loads pick the planes
@@ -243,11 +296,10 @@ struct Walker<false> {
                 const float4 nx = plane(np, onx), fx = plane(np, ofx), ny = plane(np, ony), fy = plane(np, ofy);
                 const float4 nz = plane(np, onz), fz = plane(np, ofz);
                 const int4 ch = __ldg(&np->child);
-                bool h0, h1, h2, h3;
-                float t[4] = {slab_nh(nx.x, fx.x, ny.x, fy.x, nz.x, fz.x, inv, oi, tMin, tBest, h0),
-                              slab_nh(nx.y, fx.y, ny.y, fy.y, nz.y, fz.y, inv, oi, tMin, tBest, h1),
-                              slab_nh(nx.z, fx.z, ny.z, fy.z, nz.z, fz.z, inv, oi, tMin, tBest, h2),
-                              slab_nh(nx.w, fx.w, ny.w, fy.w, nz.w, fz.w, inv, oi, tMin, tBest, h3)};
+                float t[4];
+                bool hh[4];
+                slab4_nh(nx, fx, ny, fy, nz, fz, R2, tMin, tBest, t, hh);
+                const bool h0 = hh[0], h1 = hh[1], h2 = hh[2], h3 = hh[3];
                 int c[4] = {ch.x, ch.y, ch.z, ch.w};
                 // most visits accept exactly one child (no ordering needed); two or
                 // more are sorted (rejected children last) and all but the nearest
