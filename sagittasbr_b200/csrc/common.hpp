@@ -44,12 +44,15 @@ static_assert(sizeof(GNode4) == 112, "GNode4 must be 112 bytes");
 constexpr int kLeafMax = 15;
 constexpr int kStackDepth = 64;     // reference uses 64 (src/cuda/rtKernels.cu:65)
 
-// Leaf-ordered triangle: v0, e1 = v1 - v0, e2 = v2 - v0 and the unit normal
-// unit(e1 x e2) in the w lanes (three 16 B loads).
+// Leaf-ordered triangle: the three FP32 vertices and the unit normal
+// unit(e1 x e2), e1 = v1 - v0, e2 = v2 - v0, in the w lanes (three 16 B loads).
+// Vertices rather than edges: triangles sharing an edge then hold bit-identical
+// copies of its end points, which the watertight test needs; Moller-Trumbore forms
+// the edges in the kernel with the same FP32 subtraction the reference does.
 struct __align__(16) GTri {
-    float4 p;     // v0.xyz, n.x
-    float4 e1;    // e1.xyz, n.y
-    float4 e2;    // e2.xyz, n.z
+    float4 v0;    // v0.xyz, n.x
+    float4 v1;    // v1.xyz, n.y
+    float4 v2;    // v2.xyz, n.z
 };
 
 // FP64 twin of GTri used by SBR_PREC_FP64.

@@ -111,11 +111,11 @@ __device__ __forceinline__ bool step_f(RayF& r, PolF& e, const SceneView& S, int
         tB = __uint_as_float((unsigned)(key >> 32));
         slot = (int)(unsigned)key;
     } else {
-        slot = Walker<false>::closest(S, r.o, r.d, 1.0e-3f, tB, err);
+        slot = Walker<false>::closest<PREC == SBR_PREC_MIXED>(S, r.o, r.d, 1.0e-3f, tB, err);
     }
     if (slot < 0) return true;
     const GTri* T = S.tris + slot;
-    const F3 n = f3(__ldg(&T->p.w), __ldg(&T->e1.w), __ldg(&T->e2.w));
+    const F3 n = f3(__ldg(&T->v0.w), __ldg(&T->v1.w), __ldg(&T->v2.w));
     if constexpr (POL) {
         if (r.count > 0) {  // the field left the previous hit reflected there
             e.h = pec_reflect(e.h, r.nl);

@@ -63,9 +63,9 @@ __global__ void k_refit_tris(const float* __restrict__ xyz, const uint32_t* __re
         n[2] = __fdiv_rn(nz, len);
     }
     GTri g;
-    g.p = make_float4(p[0][0], p[0][1], p[0][2], n[0]);
-    g.e1 = make_float4(e1[0], e1[1], e1[2], n[1]);
-    g.e2 = make_float4(e2[0], e2[1], e2[2], n[2]);
+    g.v0 = make_float4(p[0][0], p[0][1], p[0][2], n[0]);
+    g.v1 = make_float4(p[1][0], p[1][1], p[1][2], n[1]);
+    g.v2 = make_float4(p[2][0], p[2][1], p[2][2], n[2]);
     tris[slot] = g;
     if (tris64) {
         GTri64 h;

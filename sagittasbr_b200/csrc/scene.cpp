@@ -241,8 +241,8 @@ sbr_status sbr_scene_create(const float* xyz, size_t nverts, const uint32_t* tri
         for (size_t k = 0; k < g.size(); ++k) s->refit_nodes[(size_t)fillp[(size_t)level[k]]++] = (int32_t)k;
     }
 
-    // leaf-ordered triangles: v0, e1, e2 in FP32 (reference FP32 arithmetic) and
-    // the unit normal unit(e1 x e2) (src/cuda/rtKernels.cu:13-14,42)
+    // leaf-ordered triangles: v0, v1, v2 in FP32 and the unit normal unit(e1 x e2)
+    // with e1, e2 in the reference's FP32 arithmetic (src/cuda/rtKernels.cu:13-14,42)
     std::vector<GTri> tr(ntris);
     std::vector<int32_t> ids(ntris);
     for (size_t slot = 0; slot < ntris; ++slot) {
@@ -260,9 +260,9 @@ sbr_status sbr_scene_create(const float* xyz, size_t nverts, const uint32_t* tri
         float len = std::sqrt(nx * nx + ny * ny + nz * nz);
         float n[3] = {0.0f, 0.0f, 0.0f};
         if (len > 0.0f) { n[0] = nx / len; n[1] = ny / len; n[2] = nz / len; }
-        tr[slot].p = make_float4(a[0], a[1], a[2], n[0]);
-        tr[slot].e1 = make_float4(e1[0], e1[1], e1[2], n[1]);
-        tr[slot].e2 = make_float4(e2[0], e2[1], e2[2], n[2]);
+        tr[slot].v0 = make_float4(a[0], a[1], a[2], n[0]);
+        tr[slot].v1 = make_float4(b[0], b[1], b[2], n[1]);
+        tr[slot].v2 = make_float4(c[0], c[1], c[2], n[2]);
     }
     auto t1 = std::chrono::steady_clock::now();
     s->build_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();

@@ -414,7 +414,8 @@ __device__ __forceinline__ void raster_pixel(const GTri& T, int slot, const Segm
                                              int i, int j, unsigned long long* zbuf) {
     const F3 o = primary_origin<PREC>(G, J, i, j);
     float t;
-    if (mt_f(T, o, d, 1.0e-3f, 1e20f, t)) {
+    const bool hit = PREC == SBR_PREC_MIXED ? wt_f(T, o, wt_ray(d), 1.0e-3f, 1e20f, t) : mt_f(T, o, d, 1.0e-3f, 1e20f, t);
+    if (hit) {
         const unsigned long long key = ((unsigned long long)__float_as_uint(t) << 32) | (unsigned)slot;
         atomicMin(zbuf + G.zbase + (int64_t)(j - G.j0) * G.ni + (i - G.i0), key);
     }
@@ -424,7 +425,8 @@ __device__ __forceinline__ void raster_pixel(const GTri& T, int slot, const Segm
 // one angle are parallel and start at the pixel centres of the launcher grid, so a
 // triangle can only be hit by the rays whose pixel centres lie inside its projected
 // box (plus a small margin).  Each (segment, triangle) pair tests exactly those
-// rays with the trace's own Moller-Trumbore and keeps, per pixel, the nearest hit
+// rays with the trace's own triangle test (watertight in mixed precision,
+// Moller-Trumbore otherwise) and keeps, per pixel, the nearest hit
 // (smallest t, then smallest slot) with a 64-bit atomicMin.  Triangles covering
 // few pixels are done by one lane; larger ones are spread over the warp.
 template <int PREC>
@@ -442,11 +444,9 @@ __global__ void __launch_bounds__(256) k_raster(const RasterParams R) {
         GTri T;
         if (slot < R.ntris) {
             T = R.S.tris[slot];
-            // the triangle Moller-Trumbore sees: v0, v0 + e1, v0 + e2 (exact in FP64)
-            const double x0 = T.p.x, y0 = T.p.y, z0 = T.p.z;
-            const double X[3] = {x0, x0 + T.e1.x, x0 + T.e2.x};
-            const double Y[3] = {y0, y0 + T.e1.y, y0 + T.e2.y};
-            const double Z[3] = {z0, z0 + T.e1.z, z0 + T.e2.z};
+            const double X[3] = {T.v0.x, T.v1.x, T.v2.x};
+            const double Y[3] = {T.v0.y, T.v1.y, T.v2.y};
+            const double Z[3] = {T.v0.z, T.v1.z, T.v2.z};
             double smin = 1e300, smax = -1e300, tmin = 1e300, tmax = -1e300;
 #pragma unroll
             for (int k = 0; k < 3; ++k) {

@@ -173,12 +173,13 @@ __device__ __forceinline__ double slab_d(double lx, double hx, double ly, double
 
 // Moller-Trumbore in the reference's operation order.
 __device__ __forceinline__ bool mt_f(const GTri& T, F3 o, F3 d, float tMin, float tMax, float& t) {
-    F3 e1 = f3(T.e1.x, T.e1.y, T.e1.z), e2 = f3(T.e2.x, T.e2.y, T.e2.z);
+    const F3 v0 = f3(T.v0.x, T.v0.y, T.v0.z);
+    F3 e1 = f3(T.v1.x, T.v1.y, T.v1.z) - v0, e2 = f3(T.v2.x, T.v2.y, T.v2.z) - v0;
     F3 pv = cross(d, e2);
     float det = dot(e1, pv);
     if (fabsf(det) < 1.0e-6f) return false;
     float inv = __frcp_rn(det);
-    F3 tv = o - f3(T.p.x, T.p.y, T.p.z);
+    F3 tv = o - v0;
     float u = dot(tv, pv) * inv;
     if (u < 0.0f || u > 1.0f) return false;
     F3 qv = cross(tv, e1);
@@ -188,6 +189,96 @@ __device__ __forceinline__ bool mt_f(const GTri& T, F3 o, F3 d, float tMin, floa
     if (tt < tMin || tt > tMax) return false;
     t = tt;
     return true;
+}
+
+// Watertight ray / triangle test (Woop, Benthin and Wald, "Watertight Ray/Triangle
+// Intersection", JCGT 2(1), 2013), two-sided, FP32.  The vertices are moved to the
+// ray origin and sheared so the ray runs along the axis kz of its largest direction
+// component; the three 2-D edge functions U, V, W of the sheared triangle are then
+// formed without FMA contraction, so a shared edge evaluates to exactly opposite
+// values in its two triangles and no ray passes between them (a zero falls back to
+// FP64, where the products are exact).  Accepted as by the reference's
+// Moller-Trumbore otherwise: |det| < 1e-6 rejected (|det_MT| = |U + V + W| |d_kz|),
+// t in [tMin, tMax]; t = T / det with the approximate reciprocal (2 ulp).
+struct WtRay {
+    int kz;         // dominant axis of d; kx = kz + 1, ky = kz + 2 (mod 3)
+    float sx, sy;   // d[kx] / d[kz], d[ky] / d[kz] (to 2 ulp)
+    float sz;       // 1 / d[kz] (to 2 ulp)
+    float adz;      // |d[kz]|
+};
+__device__ __forceinline__ WtRay wt_ray(F3 d) {
+    const float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+    WtRay w;
+    w.kz = ax > ay ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+    const float dz = w.kz == 0 ? d.x : w.kz == 1 ? d.y : d.z;
+    const float dx = w.kz == 0 ? d.y : w.kz == 1 ? d.z : d.x;
+    const float dy = w.kz == 0 ? d.z : w.kz == 1 ? d.x : d.y;
+    // any per-ray constants keep the test watertight (each vertex is transformed the
+    // same way for every triangle); the approximate reciprocal is enough
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(w.sz) : "f"(dz));
+    w.sx = __fmul_rn(dx, w.sz);
+    w.sy = __fmul_rn(dy, w.sz);
+    w.adz = fabsf(dz);
+    return w;
+}
+template <int K>
+__device__ __forceinline__ float axis(const float4& v) {
+    return K == 0 ? v.x : K == 1 ? v.y : v.z;
+}
+template <int K>
+__device__ __forceinline__ float axis(F3 v) {
+    return K == 0 ? v.x : K == 1 ? v.y : v.z;
+}
+template <int KZ>
+__device__ __forceinline__ bool wt_tri(const GTri& T, F3 o, const WtRay& w, float tMin, float tMax, float& t) {
+    constexpr int KX = (KZ + 1) % 3, KY = (KZ + 2) % 3;
+    const float ox = axis<KX>(o), oy = axis<KY>(o), oz = axis<KZ>(o);
+    const float az = __fsub_rn(axis<KZ>(T.v0), oz), bz = __fsub_rn(axis<KZ>(T.v1), oz),
+                cz = __fsub_rn(axis<KZ>(T.v2), oz);
+    const float ax = __fmaf_rn(-w.sx, az, __fsub_rn(axis<KX>(T.v0), ox));
+    const float ay = __fmaf_rn(-w.sy, az, __fsub_rn(axis<KY>(T.v0), oy));
+    const float bx = __fmaf_rn(-w.sx, bz, __fsub_rn(axis<KX>(T.v1), ox));
+    const float by = __fmaf_rn(-w.sy, bz, __fsub_rn(axis<KY>(T.v1), oy));
+    const float cx = __fmaf_rn(-w.sx, cz, __fsub_rn(axis<KX>(T.v2), ox));
+    const float cy = __fmaf_rn(-w.sy, cz, __fsub_rn(axis<KY>(T.v2), oy));
+    float U = __fsub_rn(__fmul_rn(cx, by), __fmul_rn(cy, bx));
+    float V = __fsub_rn(__fmul_rn(ax, cy), __fmul_rn(ay, cx));
+    float W = __fsub_rn(__fmul_rn(bx, ay), __fmul_rn(by, ax));
+    if (U == 0.0f || V == 0.0f || W == 0.0f) {
+        U = float(__dsub_rn(__dmul_rn(cx, by), __dmul_rn(cy, bx)));
+        V = float(__dsub_rn(__dmul_rn(ax, cy), __dmul_rn(ay, cx)));
+        W = float(__dsub_rn(__dmul_rn(bx, ay), __dmul_rn(by, ax)));
+    }
+    if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+    const float det = __fadd_rn(__fadd_rn(U, V), W);
+    if (!(fabsf(det) * w.adz >= 1.0e-6f)) return false;
+    const float T3 = __fmaf_rn(U, az, __fmaf_rn(V, bz, __fmul_rn(W, cz)));
+    float rdet;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rdet) : "f"(det));
+    const float tt = __fmul_rn(__fmul_rn(T3, w.sz), rdet);
+    if (!(tt >= tMin && tt <= tMax)) return false;
+    t = tt;
+    return true;
+}
+// A leaf's triangles with the axis order fixed at compile time: the switch on kz
+// sits outside the loop, so a warp whose rays share a dominant axis runs one variant.
+template <int KZ>
+__device__ __forceinline__ void leaf_wt(const GTri* __restrict__ tris, int first, int cnt, F3 o, const WtRay& w,
+                                        float tMin, float& tBest, int& best) {
+    for (int k = 0; k < cnt; ++k) {
+        float tt;
+        if (wt_tri<KZ>(tris[first + k], o, w, tMin, tBest, tt)) {
+            tBest = tt;
+            best = first + k;
+        }
+    }
+}
+__device__ __forceinline__ bool wt_f(const GTri& T, F3 o, const WtRay& w, float tMin, float tMax, float& t) {
+    switch (w.kz) {
+        case 0: return wt_tri<0>(T, o, w, tMin, tMax, t);
+        case 1: return wt_tri<1>(T, o, w, tMin, tMax, t);
+        default: return wt_tri<2>(T, o, w, tMin, tMax, t);
+    }
 }
 
 __device__ __forceinline__ bool mt_d(const GTri64& T, D3 o, D3 d, double tMin, double tMax, double& t) {
@@ -258,11 +349,16 @@ __device__ __forceinline__ unsigned long long pack_entry(int ref, float t) {
 template <bool kF64>
 struct Walker;
 
+// The FP32 walker tests triangles with the watertight test (kWT) or with the
+// reference's Moller-Trumbore.
 template <>
 struct Walker<false> {
+    template <bool kWT>
     __device__ __forceinline__ static int closest(const SceneView& S, F3 o, F3 d, float tMin, float& tBest,
                                                   uint32_t& err) {
         const F3 inv{slab_inv(d.x), slab_inv(d.y), slab_inv(d.z)};
+        WtRay wr;
+        if constexpr (kWT) wr = wt_ray(d);
         const F3 oi{o.x * inv.x, o.y * inv.y, o.z * inv.z};
         const Slab2 R2 = slab2(inv, oi);
         // byte offsets of each axis' near and far planes within a GNode4 (lo planes
@@ -326,9 +422,17 @@ struct Walker<false> {
                 if (++iters > kIterBudget) { err |= DEV_ERR_BUDGET; return -1; }
                 const int code = ~ref;
                 const int first = code >> 4, cnt = code & 15;
-                for (int k = 0; k < cnt; ++k) {
-                    float tt;
-                    if (mt_f(S.tris[first + k], o, d, tMin, tBest, tt)) { tBest = tt; best = first + k; }
+                if constexpr (kWT) {
+                    switch (wr.kz) {
+                        case 0: leaf_wt<0>(S.tris, first, cnt, o, wr, tMin, tBest, best); break;
+                        case 1: leaf_wt<1>(S.tris, first, cnt, o, wr, tMin, tBest, best); break;
+                        default: leaf_wt<2>(S.tris, first, cnt, o, wr, tMin, tBest, best); break;
+                    }
+                } else {
+                    for (int k = 0; k < cnt; ++k) {
+                        float tt;
+                        if (mt_f(S.tris[first + k], o, d, tMin, tBest, tt)) { tBest = tt; best = first + k; }
+                    }
                 }
                 if (!pop()) return best;
             } while (ref < 0);
