@@ -451,6 +451,7 @@ def main():
                     help="let the plan time candidate work-item sizes / grid sizes on a sample first")
     ap.add_argument("--polarization", default="scalar", choices=["scalar", "hhvv"],
                     help="the reference's scalar PO term, or HH and VV fields with E-vector tracking")
+    ap.add_argument("--gpu-build", action="store_true", help="build the scene's SAH tree on the GPU")
     ap.add_argument("--no-ref-gpu", action="store_true",
                     help="skip the reference's own GPU build (baseline/_ref) on the same GPU")
     ap.add_argument("--fp64-check", type=int, default=0,
@@ -486,8 +487,9 @@ def main():
     torch.cuda.set_stream(stream)
     sp = stream.cuda_stream
     t_scene = time.perf_counter()
-    scene = sbr.Scene(w["verts"], w["tris"], device=local)
+    scene = sbr.Scene(w["verts"], w["tris"], device=local, gpu_build=args.gpu_build)
     scene_s = time.perf_counter() - t_scene
+    sah_ms = scene.info()["sah_ms"]
     job = sbr.JobSpec(w["theta"], w["phi"], w["freqs"], w["nx"], w["ny"], w["G"], w["max_bounces"], w["R"])
     first_hit = sbr.FIRST_HIT_RASTER if args.first_hit == "raster" else sbr.FIRST_HIT_TRAVERSE
     pol = sbr.POL_HHVV if args.polarization == "hhvv" else sbr.POL_SCALAR
@@ -664,6 +666,7 @@ def main():
                    "mode": "batched persistent", "precision": "mixed", "polarization": args.polarization,
                    "l2": "flushed before every step (256 MiB write inside the timed region)",
                    "parallelism": f"{ws} GPU(s), independent sweeps", "scene_build_s": scene_s,
+                   "sah_build": {"where": "gpu" if args.gpu_build else "host", "ms": sah_ms},
                    "plan_s": plan_s, "autotune": bool(args.autotune),
                    "blocks_per_item": info["blocks_per_item"], "ctas_per_sm": info["ctas_per_sm"]},
         "mray_bounces_per_s": bounces_step * ws / (step_ms * 1e-3) / 1e6,

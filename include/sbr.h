@@ -61,7 +61,9 @@ typedef struct sbr_build_opts {
     int32_t bin_count;    /* SAH bins; 0 -> 16 (bvhBuilder.hpp:15) */
     int32_t n_threads;    /* host threads for the build; 0 -> all */
     int32_t want_fp64;    /* also upload FP64 triangles (needed by SBR_PREC_FP64); -1 -> lazily */
-    int32_t reserved[3];
+    int32_t gpu_build;    /* 1: build the binary SAH tree on the GPU (same tree as the host build;
+                             triangles inside a leaf may be ordered differently) */
+    int32_t reserved[2];
 } sbr_build_opts;
 
 typedef struct sbr_scene_info {
@@ -71,9 +73,10 @@ typedef struct sbr_scene_info {
     int64_t device_bytes;     /* scene bytes resident on the device */
     double aabb_lo[3];
     double aabb_hi[3];
-    double build_ms;          /* host BVH build time */
+    double build_ms;          /* scene set-up time (BVH build, layout, upload) */
     int32_t device;
     int32_t bvh_depth;
+    double sah_ms;            /* of which the binary SAH build (host threads or GPU) */
 } sbr_scene_info;
 
 /* Copies the indexed triangle mesh (xyz: nverts*3 floats, tri_idx: ntris*3

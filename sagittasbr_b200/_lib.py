@@ -29,7 +29,8 @@ class BuildOpts(C.Structure):
         ("bin_count", C.c_int32),
         ("n_threads", C.c_int32),
         ("want_fp64", C.c_int32),
-        ("reserved", C.c_int32 * 3),
+        ("gpu_build", C.c_int32),
+        ("reserved", C.c_int32 * 2),
     ]
 
 
@@ -44,6 +45,7 @@ class SceneInfo(C.Structure):
         ("build_ms", C.c_double),
         ("device", C.c_int32),
         ("bvh_depth", C.c_int32),
+        ("sah_ms", C.c_double),
     ]
 
 

@@ -11,6 +11,8 @@
 // src/scene/bvhBuilder.cpp:245-248).
 #pragma once
 
+#include <cuda_runtime.h>
+
 #include <cstdint>
 #include <vector>
 
@@ -37,5 +39,11 @@ struct BinTree {
 
 // tri_lo/tri_hi: per-triangle boxes (3 floats each), used for the build.
 BinTree build_sah(const std::vector<float>& tri_lo, const std::vector<float>& tri_hi, const BuildOptions& opt);
+
+// The same tree built on the current CUDA device (gpu_build.cu): identical nodes,
+// boxes and leaf triangle sets; triangles inside a leaf may be in another order.
+// Returns false with the CUDA error in *err when a CUDA call fails.
+bool build_sah_gpu(const std::vector<float>& tri_lo, const std::vector<float>& tri_hi, const BuildOptions& opt,
+                   cudaStream_t stream, BinTree& out, cudaError_t* err);
 
 }  // namespace sbr

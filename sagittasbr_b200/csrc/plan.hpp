@@ -34,6 +34,7 @@ struct sbr_scene {
     cudaStream_t cancel_stream = nullptr;
     int depth = 0;
     double build_ms = 0.0;
+    double sah_ms = 0.0;
     // refit: 4-wide node indices grouped by depth (offsets per depth), their device
     // copy, and the per-triangle box scratch of a refit
     std::vector<int32_t> refit_nodes;

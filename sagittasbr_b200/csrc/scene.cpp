@@ -150,7 +150,21 @@ sbr_status sbr_scene_create(const float* xyz, size_t nverts, const uint32_t* tri
     bo.bin_count = o.bin_count > 0 ? o.bin_count : 16;
     bo.n_threads = o.n_threads;
     bo.max_leaf = kLeafMax;
-    BinTree tree = build_sah(lo, hi, bo);
+    const auto ts0 = std::chrono::steady_clock::now();
+    BinTree tree;
+    if (o.gpu_build > 0) {
+        cudaStream_t bs = nullptr;
+        cudaError_t be = cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking);
+        const bool ok = be == cudaSuccess && build_sah_gpu(lo, hi, bo, bs, tree, &be);
+        if (bs) cudaStreamDestroy(bs);
+        if (!ok) {
+            free_scene(s);
+            return cuda_fail(be, "GPU BVH build");
+        }
+    } else {
+        tree = build_sah(lo, hi, bo);
+    }
+    s->sah_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - ts0).count();
     s->order = tree.order;
     s->n_bin_nodes = (int64_t)tree.nodes.size();
     s->depth = tree.depth;
@@ -318,6 +332,7 @@ sbr_status sbr_scene_info_get(const sbr_scene* s, sbr_scene_info* out) {
     out->build_ms = s->build_ms;
     out->device = s->device;
     out->bvh_depth = s->depth;
+    out->sah_ms = s->sah_ms;
     return SBR_OK;
 }
 
