@@ -111,7 +111,7 @@ __device__ __forceinline__ bool step_f(RayF& r, PolF& e, const SceneView& S, int
         tB = __uint_as_float((unsigned)(key >> 32));
         slot = (int)(unsigned)key;
     } else {
-        slot = Walker<false>::closest<PREC == SBR_PREC_MIXED>(S, r.o, r.d, 1.0e-3f, tB, err);
+        slot = Walker<false>::closest<PREC == SBR_PREC_MIXED, !REC && !POL>(S, r.o, r.d, 1.0e-3f, tB, err);
     }
     if (slot < 0) return true;
     const GTri* T = S.tris + slot;

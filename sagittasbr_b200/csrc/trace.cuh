@@ -350,17 +350,20 @@ template <bool kF64>
 struct Walker;
 
 // The FP32 walker tests triangles with the watertight test (kWT) or with the
-// reference's Moller-Trumbore.
+// reference's Moller-Trumbore.  kF2 computes the slab planes two-wide: faster where
+// registers are free (the scalar sweep), slower where the six duplicated ray
+// constants push other state into local memory (polarised and recording walks).
 template <>
 struct Walker<false> {
-    template <bool kWT>
+    template <bool kWT, bool kF2 = true>
     __device__ __forceinline__ static int closest(const SceneView& S, F3 o, F3 d, float tMin, float& tBest,
                                                   uint32_t& err) {
         const F3 inv{slab_inv(d.x), slab_inv(d.y), slab_inv(d.z)};
         WtRay wr;
         if constexpr (kWT) wr = wt_ray(d);
         const F3 oi{o.x * inv.x, o.y * inv.y, o.z * inv.z};
-        const Slab2 R2 = slab2(inv, oi);
+        Slab2 R2;
+        if constexpr (kF2) R2 = slab2(inv, oi);
         // byte offsets of each axis' near and far planes within a GNode4 (lo planes
         // at 0 / 32 / 64, hi planes 16 bytes after them): the ray's direction signs
         // decide which plane enters a slab, so the loads pick the planes
@@ -394,7 +397,14 @@ struct Walker<false> {
                 const int4 ch = __ldg(&np->child);
                 float t[4];
                 bool hh[4];
-                slab4_nh(nx, fx, ny, fy, nz, fz, R2, tMin, tBest, t, hh);
+                if constexpr (kF2) {
+                    slab4_nh(nx, fx, ny, fy, nz, fz, R2, tMin, tBest, t, hh);
+                } else {
+                    t[0] = slab_nh(nx.x, fx.x, ny.x, fy.x, nz.x, fz.x, inv, oi, tMin, tBest, hh[0]);
+                    t[1] = slab_nh(nx.y, fx.y, ny.y, fy.y, nz.y, fz.y, inv, oi, tMin, tBest, hh[1]);
+                    t[2] = slab_nh(nx.z, fx.z, ny.z, fy.z, nz.z, fz.z, inv, oi, tMin, tBest, hh[2]);
+                    t[3] = slab_nh(nx.w, fx.w, ny.w, fy.w, nz.w, fz.w, inv, oi, tMin, tBest, hh[3]);
+                }
                 const bool h0 = hh[0], h1 = hh[1], h2 = hh[2], h3 = hh[3];
                 int c[4] = {ch.x, ch.y, ch.z, ch.w};
                 // most visits accept exactly one child (no ordering needed); two or
