@@ -100,13 +100,14 @@ __device__ __forceinline__ float slab_nf(float nx, float fx, float ny, float fy,
     const float tf = min3f(fmaf(fx, inv.x, -oi.x), fmaf(fy, inv.y, -oi.y), fminf(fmaf(fz, inv.z, -oi.z), tMax));
     return tn <= tf * kSlabSlack ? tn : __int_as_float(0x7f800000);
 }
-// slab_nf as an entry distance and an acceptance flag: `hit` is exactly
-// slab_nf(...) <= tMax, without materialising +inf for rejected boxes.
+// slab_nf as an entry distance and an acceptance flag, without materialising +inf
+// for rejected boxes: `hit` is tn <= tf (1 + 2^-20) with tf already clamped to tMax,
+// so an accepted entry lies at most 2^-20 relative beyond tMax (boxes only prune).
 __device__ __forceinline__ float slab_nh(float nx, float fx, float ny, float fy, float nz, float fz, F3 inv, F3 oi,
                                          float tMin, float tMax, bool& hit) {
     const float tn = max3f(fmaf(nx, inv.x, -oi.x), fmaf(ny, inv.y, -oi.y), fmaxf(fmaf(nz, inv.z, -oi.z), tMin));
     const float tf = min3f(fmaf(fx, inv.x, -oi.x), fmaf(fy, inv.y, -oi.y), fminf(fmaf(fz, inv.z, -oi.z), tMax));
-    hit = (tn <= tf * kSlabSlack) & (tn <= tMax);
+    hit = tn <= tf * kSlabSlack;
     return tn;
 }
 // Two-wide FP32 (sm_100 `fma.rn.f32x2`): both halves rounded exactly as fmaf, so
@@ -157,7 +158,7 @@ __device__ __forceinline__ void slab4_nh(const float4& nx, const float4& fx, con
     for (int k = 0; k < 4; ++k) {
         const float tn = max3f(xn[k], yn[k], fmaxf(zn[k], tMin));
         const float tf = min3f(xf[k], yf[k], fminf(zf[k], tMax));
-        h[k] = (tn <= tf * kSlabSlack) & (tn <= tMax);
+        h[k] = tn <= tf * kSlabSlack;
         t[k] = tn;
     }
 }
