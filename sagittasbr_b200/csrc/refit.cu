@@ -5,7 +5,7 @@
 // between the steps of a shape optimisation, where each gradient step moves the
 // vertices a little.
 //
-//   k_refit_tris   one thread per leaf slot: the triangle's FP32 data (v0, e1, e2,
+//   k_refit_tris   one thread per leaf slot: the triangle's FP32 data (v0, v1, v2,
 //                  unit normal) in exactly the host set-up's arithmetic (scene.cpp:
 //                  products and sums rounded one by one, no contraction), its FP64
 //                  twin when the scene has one, and its conservative box (covering
