@@ -7,6 +7,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <thread>
 
 #include "bvh_build.hpp"
 #include "plan.hpp"
@@ -34,6 +35,26 @@ inline void vert32(const float* xyz, uint32_t k, float sc, float out[3]) {
 // ... and in the FP64 build's: double(position) * double(scale).
 inline void vert64(const float* xyz, uint32_t k, double sc, double out[3]) {
     for (int a = 0; a < 3; ++a) out[a] = double(xyz[3 * k + a]) * sc;
+}
+
+// fn(begin, end) over [0, n) in contiguous chunks on the host's threads (every
+// element is written by exactly one thread, so the result does not depend on the
+// thread count).
+template <typename Fn>
+void parallel_for(size_t n, int threads, Fn fn) {
+    int nt = threads > 0 ? threads : (int)std::max(1u, std::thread::hardware_concurrency());
+    nt = (int)std::min<size_t>((size_t)nt, std::max<size_t>(1, n / 65536));
+    if (nt <= 1) {
+        fn(size_t(0), n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    const size_t chunk = (n + nt - 1) / nt;
+    for (int k = 0; k < nt; ++k) {
+        const size_t b = k * chunk, e = std::min(n, b + chunk);
+        if (b < e) pool.emplace_back(fn, b, e);
+    }
+    for (auto& t : pool) t.join();
 }
 
 void free_scene(sbr_scene* s) {
@@ -132,19 +153,21 @@ sbr_status sbr_scene_create(const float* xyz, size_t nverts, const uint32_t* tri
     // per-triangle conservative boxes (cover both the FP32 and FP64 vertices)
     const float sc32 = float(scale);
     std::vector<float> lo(3 * ntris), hi(3 * ntris);
-    for (size_t t = 0; t < ntris; ++t) {
-        for (int a = 0; a < 3; ++a) { lo[3 * t + a] = INFINITY; hi[3 * t + a] = -INFINITY; }
-        for (int c = 0; c < 3; ++c) {
-            float p32[3];
-            double p64[3];
-            vert32(xyz, tri_idx[3 * t + c], sc32, p32);
-            vert64(xyz, tri_idx[3 * t + c], scale, p64);
-            for (int a = 0; a < 3; ++a) {
-                lo[3 * t + a] = std::min({lo[3 * t + a], p32[a], round_down(p64[a])});
-                hi[3 * t + a] = std::max({hi[3 * t + a], p32[a], round_up(p64[a])});
+    parallel_for(ntris, o.n_threads, [&](size_t t0, size_t t1) {
+        for (size_t t = t0; t < t1; ++t) {
+            for (int a = 0; a < 3; ++a) { lo[3 * t + a] = INFINITY; hi[3 * t + a] = -INFINITY; }
+            for (int c = 0; c < 3; ++c) {
+                float p32[3];
+                double p64[3];
+                vert32(xyz, tri_idx[3 * t + c], sc32, p32);
+                vert64(xyz, tri_idx[3 * t + c], scale, p64);
+                for (int a = 0; a < 3; ++a) {
+                    lo[3 * t + a] = std::min({lo[3 * t + a], p32[a], round_down(p64[a])});
+                    hi[3 * t + a] = std::max({hi[3 * t + a], p32[a], round_up(p64[a])});
+                }
             }
         }
-    }
+    });
     BuildOptions bo;
     bo.leaf_size = o.leaf_size > 0 ? std::min(o.leaf_size, kLeafMax) : 4;
     bo.bin_count = o.bin_count > 0 ? o.bin_count : 16;
@@ -203,44 +226,50 @@ sbr_status sbr_scene_create(const float* xyz, size_t nverts, const uint32_t* tri
         struct Work {
             int32_t bin, slot, need, depth;
         };
+        g.reserve(tree.nodes.size() / 2 + 1);
+        level.reserve(tree.nodes.size() / 2 + 1);
         g.emplace_back();
         std::vector<Work> work{{0, 0, 0, 0}};
         while (!work.empty()) {
             const Work w = work.back();
             const int32_t b = w.bin, slot = w.slot;
             work.pop_back();
-            std::vector<int32_t> kids{tree.nodes[b].left, tree.nodes[b].right};
-            while (kids.size() < 4 && w.need + (int)kids.size() <= kStackDepth) {
+            int32_t kids[4] = {tree.nodes[b].left, tree.nodes[b].right, -1, -1};
+            int nk = 2;
+            while (nk < 4 && w.need + nk <= kStackDepth) {
                 int best = -1;
                 float ba = -1.0f;
-                for (size_t k = 0; k < kids.size(); ++k) {
+                for (int k = 0; k < nk; ++k) {
                     const BinNode& K = tree.nodes[kids[k]];
-                    if (K.left >= 0 && area(K) > ba) { ba = area(K); best = (int)k; }
+                    if (K.left >= 0 && area(K) > ba) { ba = area(K); best = k; }
                 }
                 if (best < 0) break;
                 const BinNode& K = tree.nodes[kids[best]];
+                for (int k = nk; k > best + 1; --k) kids[k] = kids[k - 1];
                 kids[best] = K.left;
-                kids.insert(kids.begin() + best + 1, K.right);
+                kids[best + 1] = K.right;
+                ++nk;
             }
             GNode4 n;
-            std::vector<Work> inner;
-            const int32_t need = w.need + (int32_t)kids.size() - 1;
+            Work inner[4];
+            int ni = 0;
+            const int32_t need = w.need + nk - 1;
             for (int c = 0; c < 4; ++c) {
-                if (c >= (int)kids.size()) { fill(n, c, nullptr, ~0); continue; }
+                if (c >= nk) { fill(n, c, nullptr, ~0); continue; }
                 const BinNode& K = tree.nodes[kids[c]];
                 if (K.left >= 0) {
-                    int32_t idx = (int32_t)g.size() + (int32_t)inner.size();
-                    inner.push_back({kids[c], idx, need, w.depth + 1});
+                    const int32_t idx = (int32_t)g.size() + ni;
+                    inner[ni++] = {kids[c], idx, need, w.depth + 1};
                     fill(n, c, &K, idx);
                 } else {
                     fill(n, c, &K, leafRef(K));
                 }
             }
             g[slot] = n;
-            g.resize(g.size() + inner.size());
+            g.resize(g.size() + ni);
             level.resize(g.size());
-            for (const Work& q : inner) level[q.slot] = q.depth;
-            for (auto it = inner.rbegin(); it != inner.rend(); ++it) work.push_back(*it);
+            for (int q = 0; q < ni; ++q) level[inner[q].slot] = inner[q].depth;
+            for (int q = ni - 1; q >= 0; --q) work.push_back(inner[q]);
         }
     }
     s->n_gnodes = (int64_t)g.size();
@@ -259,25 +288,27 @@ sbr_status sbr_scene_create(const float* xyz, size_t nverts, const uint32_t* tri
     // with e1, e2 in the reference's FP32 arithmetic (src/cuda/rtKernels.cu:13-14,42)
     std::vector<GTri> tr(ntris);
     std::vector<int32_t> ids(ntris);
-    for (size_t slot = 0; slot < ntris; ++slot) {
-        int32_t t = s->order[slot];
-        ids[slot] = t;
-        float a[3], b[3], c[3];
-        vert32(xyz, tri_idx[3 * t], sc32, a);
-        vert32(xyz, tri_idx[3 * t + 1], sc32, b);
-        vert32(xyz, tri_idx[3 * t + 2], sc32, c);
-        float e1[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
-        float e2[3] = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
-        float nx = e1[1] * e2[2] - e1[2] * e2[1];
-        float ny = -(e1[0] * e2[2] - e1[2] * e2[0]);
-        float nz = e1[0] * e2[1] - e1[1] * e2[0];
-        float len = std::sqrt(nx * nx + ny * ny + nz * nz);
-        float n[3] = {0.0f, 0.0f, 0.0f};
-        if (len > 0.0f) { n[0] = nx / len; n[1] = ny / len; n[2] = nz / len; }
-        tr[slot].v0 = make_float4(a[0], a[1], a[2], n[0]);
-        tr[slot].v1 = make_float4(b[0], b[1], b[2], n[1]);
-        tr[slot].v2 = make_float4(c[0], c[1], c[2], n[2]);
-    }
+    parallel_for(ntris, o.n_threads, [&](size_t s0, size_t s1) {
+        for (size_t slot = s0; slot < s1; ++slot) {
+            int32_t t = s->order[slot];
+            ids[slot] = t;
+            float a[3], b[3], c[3];
+            vert32(xyz, tri_idx[3 * t], sc32, a);
+            vert32(xyz, tri_idx[3 * t + 1], sc32, b);
+            vert32(xyz, tri_idx[3 * t + 2], sc32, c);
+            float e1[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+            float e2[3] = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
+            float nx = e1[1] * e2[2] - e1[2] * e2[1];
+            float ny = -(e1[0] * e2[2] - e1[2] * e2[0]);
+            float nz = e1[0] * e2[1] - e1[1] * e2[0];
+            float len = std::sqrt(nx * nx + ny * ny + nz * nz);
+            float n[3] = {0.0f, 0.0f, 0.0f};
+            if (len > 0.0f) { n[0] = nx / len; n[1] = ny / len; n[2] = nz / len; }
+            tr[slot].v0 = make_float4(a[0], a[1], a[2], n[0]);
+            tr[slot].v1 = make_float4(b[0], b[1], b[2], n[1]);
+            tr[slot].v2 = make_float4(c[0], c[1], c[2], n[2]);
+        }
+    });
     auto t1 = std::chrono::steady_clock::now();
     s->build_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
 
