@@ -57,7 +57,8 @@ typedef struct sbr_scene sbr_scene;
 typedef struct sbr_build_opts {
     double model_scale;   /* vertices are multiplied by this (--model-scale, rtRcsEntry.cu:137-145); 0 -> 1 */
     int32_t device;       /* CUDA device ordinal; -1 -> current device */
-    int32_t leaf_size;    /* max triangles per BVH leaf; 0 -> 4 (bvhBuilder.hpp:14) */
+    int32_t leaf_size;    /* max triangles per BVH leaf; 0 -> 3 (the reference's builder uses 4,
+                             bvhBuilder.hpp:14; 3 traces faster with 4-wide nodes) */
     int32_t bin_count;    /* SAH bins; 0 -> 16 (bvhBuilder.hpp:15) */
     int32_t n_threads;    /* host threads for the build; 0 -> all */
     int32_t want_fp64;    /* also upload FP64 triangles (needed by SBR_PREC_FP64); -1 -> lazily */
