@@ -35,8 +35,8 @@ All meshes are synthetic and seeded; no dataset is involved.
 `roofline`   dominant kernel (k_trace): algorithmic FP32 work per closest-hit query
              on the reference SAH tree, 27 V_box + 57 V_tri FLOP, V_box / V_tri counted
              by the instrumented CPU oracle on a sample of the same sweep; peak = FP32
-             SGEMM throughput measured in the same run (the driver's peak file has
-             HBM and bf16 only).
+             SGEMM throughput measured in the same run (MEASURED_PEAKS.json holds
+             HBM and bf16 figures only).
 `cpu_baseline` the reference's own per-ray routine (src/cuda/rtKernels.cu) compiled
              for the host (oracle/_ref), OpenMP over all host cores, timed on a bounded
              random sample of (angle, frequency) samples of the same sweep.
