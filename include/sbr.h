@@ -43,7 +43,7 @@ typedef int32_t sbr_status;
 #define SBR_ERR_CANCELLED 11    /* sbr_scene_cancel() observed by the kernel  */
 #define SBR_ERR_IO 12           /* file could not be read / written           */
 #define SBR_ERR_PARSE 13        /* malformed model / config file             */
-#define SBR_ERR_UNSUPPORTED 14  /* option not available in this build         */
+#define SBR_ERR_UNSUPPORTED 14  /* option or combination not supported          */
 
 /* Short name of a status code (static string). */
 const char* sbr_status_str(sbr_status s);
