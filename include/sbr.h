@@ -159,7 +159,7 @@ typedef struct sbr_run_opts {
     void* stream;             /* cudaStream_t to launch on; NULL -> the scene's own stream */
     int32_t ctas_per_sm;      /* persistent grid size per SM; 0 -> occupancy-derived */
     int32_t first_hit;        /* SBR_FIRST_HIT_* */
-    int32_t blocks_per_item;  /* 8x4-ray blocks per work item; 0 -> automatic (batched: blocks / 1024
+    int32_t blocks_per_item;  /* 32-ray blocks (4 x 8) per work item; 0 -> automatic (batched: blocks / 1024
                                  clamped to 1..8 per angle, per-angle mode: 1) */
     int32_t autotune;         /* 1: sbr_plan_create times candidate (blocks_per_item, ctas_per_sm)
                                  settings on a sample of the plan's angles and keeps the fastest

@@ -218,11 +218,11 @@ __global__ void __launch_bounds__(kCtaThreads, 6) k_adjoint(const AdjointParams 
         for (int k = 0; k < K; ++k) gk[k] = 0.0;
         const int b0 = int(item - G.item_base) * G.blocks_per_item;
         const int nslots = min(G.blocks_per_item, G.blocks - b0) * 32;
-        for (int s0 = 0; s0 < nslots; s0 += 32) {  // one 8x4 ray block per step, all lanes
+        for (int s0 = 0; s0 < nslots; s0 += 32) {  // one 4x8 ray block per step, all lanes
             const int s = s0 + lane;
             const int blk = b0 + (s >> 5), l = s & 31;
-            const int i = G.i0 + (blk % G.blocks_x) * kBlockW + (l & 7);
-            const int j = G.j0 + (blk / G.blocks_x) * kBlockH + (l >> 3);
+            const int i = G.i0 + (blk % G.blocks_x) * kBlockW + (l % kBlockW);
+            const int j = G.j0 + (blk / G.blocks_x) * kBlockH + (l / kBlockW);
             adjoint_ray<PREC>(P, G, J, F, K, cot, i, j, i < G.i0 + G.ni && j < G.j0 + G.nj, gk, err);
         }
         // lanes -> warp in a fixed order, one atomic per (item, frequency)

@@ -1,8 +1,8 @@
 // trace.cu -- sm_100a kernels of the SBR hot path and the plan that launches them.
 //
-// One work item = a run of 8x4-ray blocks of one (job, angle) segment, owned by
+// One work item = a run of 4x8-ray blocks of one (job, angle) segment, owned by
 // one warp.  Warps take items from a device queue (persistent grid), trace one
-// 8x4 block of parallel rays at a time through every bounce (trace.cuh), and fold
+// 4x8 block of parallel rays at a time through every bounce (trace.cuh), and fold
 // the PO exit-ray term of every frequency of the job into per-lane FP64 sums.  At the end of an item the warp reduces them in
 // a fixed order and adds the total, quantised to a per-frequency fixed-point unit,
 // to int64 accumulators with atomicAdd.  Integer addition is associative, so the
@@ -179,7 +179,7 @@ __device__ __forceinline__ void add_fixed(unsigned long long* acc, double v, dou
 }
 
 // Warp-persistent sweep kernel.  Every warp independently takes a work item (a
-// run of 8x4-ray blocks of one (job, angle) segment) and traces it one block at a
+// run of 4x8-ray blocks of one (job, angle) segment) and traces it one block at a
 // time, all lanes at the same bounce (no CTA-wide barrier anywhere).  Each lane
 // folds the PO terms of its finished rays into FP64 sums; at the end of the item
 // the warp reduces them in a fixed order and adds the total, as int64 fixed
@@ -244,8 +244,8 @@ __global__ void __launch_bounds__(kCtaThreads, kMinCtasPerSm) k_trace(const Trac
                 const int s = next + __popc(need & ((1u << lane) - 1u));
                 if (!active && s < nslots) {
                     const int blk = b0 + (s >> 5), l = s & 31;
-                    const int i = G.i0 + (blk % G.blocks_x) * kBlockW + (l & 7);
-                    const int j = G.j0 + (blk / G.blocks_x) * kBlockH + (l >> 3);
+                    const int i = G.i0 + (blk % G.blocks_x) * kBlockW + (l % kBlockW);
+                    const int j = G.j0 + (blk / G.blocks_x) * kBlockH + (l / kBlockW);
                     if (i < i_end && j < j_end) {
                         if (F64) start_d(rd, G, J, i, j);
                         else start_f<PREC>(rf, G, J, i, j);
@@ -343,7 +343,7 @@ __global__ void __launch_bounds__(kCtaThreads, kMinCtasPerSm) k_trace(const Trac
                     }
                 }
             }
-            // the next 8x4 block starts when the whole warp is done with this one:
+            // the next 4x8 block starts when the whole warp is done with this one:
             // keeping the warp's rays at the same bounce keeps them coherent (they
             // share direction and walk the same nodes), which is worth more than
             // refilling idle lanes
