@@ -200,3 +200,13 @@ def test_scene_requires_gpu_or_reports_cleanly():
         with pytest.raises(sbr.SbrError) as e:
             sbr.Scene(v, t)
         assert e.value.status == 8  # SBR_ERR_NO_DEVICE
+
+
+def test_reference_gpu_build_loads():
+    """The reference's own GPU sweep (built into baseline/_ref by baseline/Makefile
+    where the reference tree is present) loads and reports its precision."""
+    from baseline import ref_gpu
+    for bits in (32, 64):
+        if not ref_gpu.available(bits):
+            pytest.skip("reference GPU build not present")
+        assert ref_gpu.lib(bits).sbrref_gpu_real_bits() == bits
