@@ -194,6 +194,14 @@ __global__ void __launch_bounds__(kCtaThreads, kMinCtasPerSm) k_trace(const Trac
     constexpr int NPOL = POL ? 2 : 1;
     const int lane = threadIdx.x & 31;
     const int warp_global = (int)((blockIdx.x * (unsigned)kCtaThreads + threadIdx.x) >> 5);
+    // Polarised transposed epilogues keep each lane's channel sums in shared memory
+    // (lane-owned, no atomics), leaving registers to the walk, which holds the E
+    // vectors too: +4 % on the 128-channel aircraft HH + VV sweep.  The scalar
+    // transposed epilogue keeps them in registers (shared sums measured 8 % slower
+    // on the 64-frequency aircraft).
+    constexpr bool SACC = TRANSPOSED && POL;
+    __shared__ double2 s_acc[SACC ? (kCtaThreads / 32) * NACC * 32 : 1];
+    double2* const my_acc = s_acc + (SACC ? (threadIdx.x >> 5) * NACC * 32 + lane : 0);
     const int rep = warp_global % P.n_rep;
     uint32_t err = 0;
     int iter = 0;
@@ -222,9 +230,12 @@ __global__ void __launch_bounds__(kCtaThreads, kMinCtasPerSm) k_trace(const Trac
         const int i_end = G.i0 + G.ni, j_end = G.j0 + G.nj;
         const int KC = K * NPOL;  // channels of this item
 
-        double accRe[NACC], accIm[NACC];
+        double accRe[SACC ? 1 : NACC], accIm[SACC ? 1 : NACC];
 #pragma unroll
-        for (int c = 0; c < NACC; ++c) { accRe[c] = 0.0; accIm[c] = 0.0; }
+        for (int c = 0; c < NACC; ++c) {
+            if constexpr (SACC) my_acc[c * 32] = make_double2(0.0, 0.0);
+            else { accRe[c] = 0.0; accIm[c] = 0.0; }
+        }
         unsigned cRays = 0, cHit = 0, cBounce = 0, cQuery = 0;
 
         RayF rf;
@@ -337,7 +348,8 @@ __global__ void __launch_bounds__(kCtaThreads, kMinCtasPerSm) k_trace(const Trac
                     for (int c = 0; c < NACC; ++c) {
                         const int ch = c * 32 + lane;
                         if (ch < KC) {
-                            if constexpr (POL) po_term_pol(PREC, F[ch >> 1], q.Lp, q.pa[ch & 1], accRe[c], accIm[c]);
+                            if constexpr (SACC) po_term_pol(PREC, F[ch >> 1], q.Lp, q.pa[ch & 1], my_acc[c * 32].x, my_acc[c * 32].y);
+                            else if constexpr (POL) po_term_pol(PREC, F[ch >> 1], q.Lp, q.pa[ch & 1], accRe[c], accIm[c]);
                             else po_term(PREC, F[ch], q, accRe[c], accIm[c]);
                         }
                     }
@@ -378,8 +390,8 @@ __global__ void __launch_bounds__(kCtaThreads, kMinCtasPerSm) k_trace(const Trac
                 if (ch < KC) {
                     const double invQ = fold_factor<PREC>(F[POL ? ch >> 1 : ch]);
                     unsigned long long* A = P.acc + 2 * ((cbase + ch) * P.n_rep + rep);
-                    add_fixed(A, accRe[c], invQ);
-                    add_fixed(A + 1, accIm[c], invQ);
+                    add_fixed(A, SACC ? my_acc[c * 32].x : accRe[c], invQ);
+                    add_fixed(A + 1, SACC ? my_acc[c * 32].y : accIm[c], invQ);
                 }
             }
         }
