@@ -237,6 +237,14 @@ typedef struct sbr_ray_record {
 sbr_status sbr_trace_records(sbr_scene* scene, const sbr_job* job, const sbr_run_opts* opts,
                              sbr_ray_record* out);
 
+/* Traces only the listed rays of one job, rays[3k .. 3k+2] = (angle index, i, j),
+ * with the sweep's own walk and arithmetic, and writes one record per listed ray to
+ * the host array `out` -- for per-ray checks on grids too large to record whole
+ * (no counterpart in the reference).  A listed ray outside the job's angles or grid
+ * returns SBR_ERR_INVALID_ARG before anything runs. */
+sbr_status sbr_trace_ray_list(sbr_scene* scene, const sbr_job* job, const sbr_run_opts* opts, const int32_t* rays,
+                              size_t n_rays, sbr_ray_record* out);
+
 /* ----------------------------------------------------------------- adjoint */
 /* No counterpart in the reference (its sweep is not differentiable).
  *

@@ -23,6 +23,7 @@ thread_local ref_shim_dim3 blockDim;
 #include "cuda/rtKernels.cu"
 #include "scene/bvhBuilder.cpp"
 
+#include <algorithm>
 #include <cstdint>
 #include <cstring>
 #include <vector>
@@ -198,6 +199,99 @@ int ref_sweep(const float* xyz, int64_t nverts, const uint32_t* idx, int64_t ntr
             }
         }
     }
+    return 0;
+}
+
+
+// ---- bounded samples of a sweep for the CPU baseline: the reference tree is built
+// once per scene handle, then whole ray rows of chosen (angle, grid, frequency)
+// samples are traced with the reference's own per-ray routine.
+
+typedef struct ref_scene_h {
+    bvhBuildResult tree;
+} ref_scene_h;
+
+void* ref_scene_create(const float* xyz, int64_t nverts, const uint32_t* idx, int64_t ntris, double modelScale) {
+    bool ok;
+    ref_scene_h* h = new ref_scene_h{ref_tree(xyz, nverts, idx, ntris, modelScale, ok)};
+    if (!ok) {
+        delete h;
+        return nullptr;
+    }
+    return h;
+}
+
+void ref_scene_destroy(void* h) { delete static_cast<ref_scene_h*>(h); }
+
+// Row k of the list is row j = rows[3k+2] of the n x n launcher (n = rows[3k+1]) of
+// angle rows[3k], traced at frequency freqHz[k].  The routine is called with a one-row
+// grid whose vertical edge is twice the row offset v V of the full grid, so its
+// origins llc + u U + 0.5 (2 v V) equal the full grid's bit for bit without the
+// nx*ny hit arrays of the full grid.  OpenMP over rows (dynamic); outRe/outIm get each
+// row's PO sum (src/cuda/poKernels.cu:81-109) and *seconds the wall time of the
+// traced rows (tree build excluded).  Returns 0 on success.
+int ref_trace_rows(void* handle, const double* thetaDeg, const double* phiDeg, int64_t nAngles, const int32_t* rows,
+                   int64_t nRows, const double* freqHz, double gridSize, int32_t maxBounces, double reflConst,
+                   int32_t nThreads, double* outRe, double* outIm, uint64_t* raysOut, uint64_t* bouncesOut,
+                   double* seconds) {
+    ref_scene_h* h = static_cast<ref_scene_h*>(handle);
+    if (!h || nRows < 0 || nAngles <= 0) return 1;
+    int32_t nmax = 1;
+    for (int64_t k = 0; k < nRows; ++k) {
+        const int32_t a = rows[3 * k], n = rows[3 * k + 1], j = rows[3 * k + 2];
+        if (a < 0 || a >= nAngles || n <= 0 || j < 0 || j >= n || !(freqHz[k] > 0)) return 3;
+        nmax = std::max(nmax, n);
+    }
+#ifdef _OPENMP
+    if (nThreads > 0) omp_set_num_threads(nThreads);
+#endif
+    const Real G = Real(gridSize);
+    const Real c0 = REAL_CONST(299792458.0);
+    uint64_t rays = 0, bounces = 0;
+    const double t0 = omp_get_wtime();
+#pragma omp parallel reduction(+ : rays, bounces)
+    {
+        std::vector<vec3> hitNormal(nmax), lastDir(nmax);
+        std::vector<Real> hitDist(nmax);
+        std::vector<int> hitCount(nmax);
+        blockDim = {1, 1, 1};
+        threadIdx = {0, 0, 0};
+#pragma omp for schedule(dynamic)
+        for (int64_t k = 0; k < nRows; ++k) {
+            const int32_t a = rows[3 * k], n = rows[3 * k + 1], j = rows[3 * k + 2];
+            RefFrame fr = ref_frame(thetaDeg[a], phiDeg[a], G);
+            const Real v = (j + REAL_CONST(0.5)) / Real(n);
+            const vec3 vert2 = (v * fr.v) * REAL_CONST(2.0);
+            for (int32_t i = 0; i < n; ++i) {
+                blockIdx = {(unsigned)i, 0u, 0u};
+                launchRaysMultiBounce(hitNormal.data(), lastDir.data(), hitDist.data(), hitCount.data(), n, 1, fr.llc,
+                                      fr.u, vert2, fr.rayDir, h->tree.triangles.data(), h->tree.nodes.data(),
+                                      h->tree.rootIndex, maxBounces);
+            }
+            const Real kk = REAL_CONST(2.0) * Real(M_PI) / (c0 / Real(freqHz[k]));
+            const Real rayArea = (G * G) / Real(int64_t(n) * int64_t(n));
+            double re = 0, im = 0;
+            for (int32_t i = 0; i < n; ++i) {
+                const int cnt = hitCount[i];
+                bounces += (uint64_t)cnt;
+                if (cnt <= 0) continue;
+                Real Rn = REAL_CONST(1.0);
+                for (int q = 0; q < cnt; ++q) Rn *= Real(reflConst);
+                Real cosT = dot(hitNormal[i], -lastDir[i]);
+                if (!(cosT > REAL_CONST(0.0))) continue;
+                Real phase = std::fmod(REAL_CONST(2.0) * kk * hitDist[i], REAL_CONST(2.0) * Real(M_PI));
+                Real mag = (kk * rayArea / (REAL_CONST(4.0) * Real(M_PI))) * REAL_CONST(2.0) * cosT * Rn;
+                re += double(-mag * std::sin(phase));
+                im += double(mag * std::cos(phase));
+            }
+            rays += (uint64_t)n;
+            if (outRe) outRe[k] = re;
+            if (outIm) outIm[k] = im;
+        }
+    }
+    if (seconds) *seconds = omp_get_wtime() - t0;
+    if (raysOut) *raysOut = rays;
+    if (bouncesOut) *bouncesOut = bounces;
     return 0;
 }
 

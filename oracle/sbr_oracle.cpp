@@ -391,6 +391,50 @@ Frame<R> make_frame(double thetaDeg, double phiDeg, R G) {
     return f;
 }
 
+// Origin of the ray of pixel (i, j) on an nx x ny launcher (src/cuda/rtKernels.cu:118-123).
+template <class R>
+V3<R> ray_origin(const Frame<R>& fr, int32_t i, int32_t j, int32_t nx, int32_t ny) {
+    R u = (R(i) + R(0.5)) / R(nx);
+    R v = (R(j) + R(0.5)) / R(ny);
+    return fr.llc + scale(u, fr.u) + scale(v, fr.v);
+}
+
+// What one ray leaves after its bounce loop.
+template <class R>
+struct RayTrace {
+    int32_t count = 0;  // successful reflections
+    int32_t amb = 0;    // ambiguity flags OR-ed over the queries (brute force with wantAmb)
+    R dist = R(0);      // summed path
+    V3<R> nLast, dLast;
+    int32_t ids[ORACLE_MAX_REC];
+    uint64_t queries = 0;
+};
+
+// The bounce loop of one ray (src/cuda/rtKernels.cu:126-158): closest hit with
+// tMin = 1e-3, reflect, nudge 1e-4 along the normal, stop on a miss.
+template <class R>
+void trace_ray(const std::vector<Tri<R>>& tris, const std::vector<Node<R>>& nodes, const std::vector<Tri<R>>& original,
+               int32_t accel, bool wantAmb, V3<R> o, V3<R> d, int32_t maxBounces, double dEdge, double dT, double dDet,
+               RayTrace<R>& rt, Counters& cnt) {
+    const R tMin = R(0.001), tMax = R(1e20), nudge = R(1e-4);
+    for (int q = 0; q < ORACLE_MAX_REC; ++q) rt.ids[q] = -1;
+    for (int32_t b = 0; b < maxBounces; ++b) {
+        Hit<R> h;
+        rt.queries++;
+        bool hit = accel == 1 ? walk_tree(tris, nodes, o, d, tMin, tMax, h, cnt)
+                              : walk_all(original, o, d, tMin, tMax, h, cnt);
+        if (wantAmb && accel == 0) rt.amb |= ambiguity(original, o, d, hit, h, double(tMin), dEdge, dT, dDet);
+        if (!hit) break;
+        rt.nLast = h.n;
+        rt.dLast = d;
+        if (rt.count < ORACLE_MAX_REC) rt.ids[rt.count] = h.id;
+        rt.count++;
+        rt.dist += h.t;
+        d = unit(d - scale(R(2.0) * dot(d, h.n), h.n));
+        o = h.p + scale(nudge, h.n);
+    }
+}
+
 template <class R>
 int sweep_impl(const float* xyz, int64_t nverts, const uint32_t* idx, int64_t ntris, double modelScale,
                const double* thetaDeg, const double* phiDeg, int64_t nAngles, const double* freqHz,
@@ -415,7 +459,6 @@ int sweep_impl(const float* xyz, int64_t nverts, const uint32_t* idx, int64_t nt
 #endif
     const R G = R(gridSize);
     const R c0 = R(299792458.0);
-    const R tMin = R(0.001), tMax = R(1e20), nudge = R(1e-4);
     const R rayArea = (G * G) / R(int64_t(nx) * int64_t(ny));
     std::vector<R> kk(nFreqs);
     for (int64_t f = 0; f < nFreqs; ++f) kk[f] = R(2.0) * R(M_PI) / (c0 / R(freqHz[f]));
@@ -432,31 +475,14 @@ int sweep_impl(const float* xyz, int64_t nverts, const uint32_t* idx, int64_t nt
             uint64_t hitRays = 0, bounces = 0, queries = 0;
             std::vector<double> accRe(nFreqs, 0.0), accIm(nFreqs, 0.0);
             for (int32_t i = 0; i < nx; ++i) {
-                R u = (R(i) + R(0.5)) / R(nx);
-                R v = (R(j) + R(0.5)) / R(ny);
-                V3<R> o = fr.llc + scale(u, fr.u) + scale(v, fr.v);
-                V3<R> d = fr.rayDir;
-                int32_t count = 0;
-                R dist = R(0);
-                V3<R> nLast, dLast;
-                int32_t amb = 0;
-                int32_t ids[ORACLE_MAX_REC];
-                for (int q = 0; q < ORACLE_MAX_REC; ++q) ids[q] = -1;
-                for (int32_t b = 0; b < maxBounces; ++b) {
-                    Hit<R> h;
-                    queries++;
-                    bool hit = accel == 1 ? walk_tree(tris, tb.nodes, o, d, tMin, tMax, h, cnt)
-                                          : walk_all(original, o, d, tMin, tMax, h, cnt);
-                    if (rays && accel == 0) amb |= ambiguity(original, o, d, hit, h, double(tMin), dEdge, dT, dDet);
-                    if (!hit) break;
-                    nLast = h.n;
-                    dLast = d;
-                    if (count < ORACLE_MAX_REC) ids[count] = h.id;
-                    count++;
-                    dist += h.t;
-                    d = unit(d - scale(R(2.0) * dot(d, h.n), h.n));
-                    o = h.p + scale(nudge, h.n);
-                }
+                RayTrace<R> rt;
+                trace_ray(tris, tb.nodes, original, accel, rays != nullptr, ray_origin(fr, i, j, nx, ny), fr.rayDir,
+                          maxBounces, dEdge, dT, dDet, rt, cnt);
+                queries += rt.queries;
+                const int32_t count = rt.count, amb = rt.amb;
+                const R dist = rt.dist;
+                const V3<R> nLast = rt.nLast, dLast = rt.dLast;
+                const int32_t* ids = rt.ids;
                 if (count > 0) {
                     hitRays++;
                     bounces += (uint64_t)count;
@@ -513,6 +539,81 @@ int sweep_impl(const float* xyz, int64_t nverts, const uint32_t* idx, int64_t nt
             counts[a].box_tests = cBox;
             counts[a].tri_tests = cTri;
         }
+    }
+    return 0;
+}
+
+// Explicit ray list: ray k is pixel (i, j) = (rays[3k+1], rays[3k+2]) of the nx x ny
+// launcher of angle rays[3k], traced as oracle_sweep traces it.  One record per ray
+// (ambiguity flags with brute force) and the totals over the list in counts[0].
+template <class R>
+int trace_list_impl(const float* xyz, int64_t nverts, const uint32_t* idx, int64_t ntris, double modelScale,
+                    const double* thetaDeg, const double* phiDeg, int64_t nAngles, const int32_t* rayList,
+                    int64_t nRays, int32_t nx, int32_t ny, double gridSize, int32_t maxBounces, int32_t accel,
+                    int32_t nThreads, oracle_ray* rays, oracle_counts* counts, double dEdge, double dT, double dDet) {
+    if (ntris <= 0 || nverts <= 0 || nx <= 0 || ny <= 0 || nAngles <= 0 || nRays < 0) return 1;
+    for (int64_t k = 0; k < nRays; ++k) {
+        const int32_t a = rayList[3 * k], i = rayList[3 * k + 1], j = rayList[3 * k + 2];
+        if (a < 0 || a >= nAngles || i < 0 || i >= nx || j < 0 || j >= ny) return 3;
+    }
+    std::vector<Tri<R>> tris(ntris);
+    const R sc = R(modelScale);
+    for (int64_t i = 0; i < ntris; ++i) {
+        uint32_t a = idx[3 * i], b = idx[3 * i + 1], c = idx[3 * i + 2];
+        if (a >= nverts || b >= nverts || c >= nverts) return 2;
+        auto P = [&](uint32_t k) { return V3<R>(R(xyz[3 * k]) * sc, R(xyz[3 * k + 1]) * sc, R(xyz[3 * k + 2]) * sc); };
+        tris[i] = Tri<R>{P(a), P(b), P(c), (int32_t)i};
+    }
+    std::vector<Tri<R>> original = tris;
+    TreeBuilder<R> tb(tris);
+    if (accel == 1) tb.run();
+#ifdef _OPENMP
+    if (nThreads > 0) omp_set_num_threads(nThreads);
+#endif
+    std::vector<Frame<R>> frames(nAngles);
+    for (int64_t a = 0; a < nAngles; ++a) frames[a] = make_frame<R>(thetaDeg[a], phiDeg[a], R(gridSize));
+    std::atomic<uint64_t> cHit{0}, cBounce{0}, cQuery{0}, cBox{0}, cTri{0};
+#pragma omp parallel
+    {
+        Counters cnt;
+        uint64_t hitRays = 0, bounces = 0, queries = 0;
+#pragma omp for schedule(dynamic, 16)
+        for (int64_t k = 0; k < nRays; ++k) {
+            const Frame<R>& fr = frames[rayList[3 * k]];
+            RayTrace<R> rt;
+            trace_ray(tris, tb.nodes, original, accel, rays != nullptr,
+                      ray_origin(fr, rayList[3 * k + 1], rayList[3 * k + 2], nx, ny), fr.rayDir, maxBounces, dEdge,
+                      dT, dDet, rt, cnt);
+            queries += rt.queries;
+            hitRays += rt.count > 0;
+            bounces += (uint64_t)rt.count;
+            if (rays) {
+                oracle_ray& rr = rays[k];
+                rr.count = rt.count;
+                rr.amb = rt.amb;
+                rr.dist = double(rt.dist);
+                rr.normal[0] = rt.count ? double(rt.nLast.x) : 0.0;
+                rr.normal[1] = rt.count ? double(rt.nLast.y) : 0.0;
+                rr.normal[2] = rt.count ? double(rt.nLast.z) : 0.0;
+                rr.lastdir[0] = rt.count ? double(rt.dLast.x) : 0.0;
+                rr.lastdir[1] = rt.count ? double(rt.dLast.y) : 0.0;
+                rr.lastdir[2] = rt.count ? double(rt.dLast.z) : 0.0;
+                for (int q = 0; q < ORACLE_MAX_REC; ++q) rr.tri[q] = rt.ids[q];
+            }
+        }
+        cHit += hitRays;
+        cBounce += bounces;
+        cQuery += queries;
+        cBox += cnt.box;
+        cTri += cnt.tri;
+    }
+    if (counts) {
+        counts[0].rays = (uint64_t)nRays;
+        counts[0].hit_rays = cHit;
+        counts[0].bounces = cBounce;
+        counts[0].queries = cQuery;
+        counts[0].box_tests = cBox;
+        counts[0].tri_tests = cTri;
     }
     return 0;
 }
@@ -651,6 +752,20 @@ int oracle_sweep(const float* xyz, int64_t nverts, const uint32_t* idx, int64_t 
     return sweep_impl<double>(xyz, nverts, idx, ntris, modelScale, thetaDeg, phiDeg, nAngles, freqHz, nFreqs, nx, ny,
                               gridSize, maxBounces, reflConst, accel, nThreads, outRe, outIm, counts, rays, dEdge, dT,
                               dDet);
+}
+
+// Traces an explicit list of rays (see trace_list_impl); precision 64 or 32, accel
+// as oracle_sweep.  Returns 0 on success, 3 for a ray outside the angles or grid.
+int oracle_trace_rays(const float* xyz, int64_t nverts, const uint32_t* idx, int64_t ntris, double modelScale,
+                      const double* thetaDeg, const double* phiDeg, int64_t nAngles, const int32_t* rayList,
+                      int64_t nRays, int32_t nx, int32_t ny, double gridSize, int32_t maxBounces, int32_t precision,
+                      int32_t accel, int32_t nThreads, oracle_ray* rays, oracle_counts* counts, double dEdge,
+                      double dT, double dDet) {
+    if (precision == 32)
+        return trace_list_impl<float>(xyz, nverts, idx, ntris, modelScale, thetaDeg, phiDeg, nAngles, rayList, nRays,
+                                      nx, ny, gridSize, maxBounces, accel, nThreads, rays, counts, dEdge, dT, dDet);
+    return trace_list_impl<double>(xyz, nverts, idx, ntris, modelScale, thetaDeg, phiDeg, nAngles, rayList, nRays, nx,
+                                   ny, gridSize, maxBounces, accel, nThreads, rays, counts, dEdge, dT, dDet);
 }
 
 // Builds the reference SAH tree (FP64) and returns node count; when the output

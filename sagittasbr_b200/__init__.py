@@ -307,6 +307,18 @@ def trace_records(scene: Scene, job: JobSpec, precision=PREC_MIXED, first_hit=No
     return out
 
 
+def trace_ray_list(scene: Scene, job: JobSpec, rays, precision=PREC_MIXED) -> np.ndarray:
+    """Hit records [n] of the listed rays only, rays[k] = (angle index, i, j)
+    (sbr_trace_ray_list)."""
+    jc = job.to_c()
+    rl = np.ascontiguousarray(rays, dtype=np.int32).reshape(-1, 3)
+    out = np.zeros(rl.shape[0], dtype=RAY_RECORD)
+    o = _opts(MODE_BATCHED, precision)
+    check(lib().sbr_trace_ray_list(scene.handle, C.byref(jc), C.byref(o), _p(rl), rl.shape[0], _p(out)),
+          "sbr_trace_ray_list")
+    return out
+
+
 # ------------------------------------------------------------ entry surface
 def load_config(path: str = "config.txt", argv: Sequence[str] = ()) -> dict:
     """loadConfig(path, argc, argv): argv excludes the program name."""

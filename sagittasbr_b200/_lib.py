@@ -161,6 +161,7 @@ SIGNATURES = {
     "sbr_plan_destroy": (_I32, [_P]),
     "sbr_run": (_I32, [_P, _P, _SZ, _P, _P]),
     "sbr_trace_records": (_I32, [_P, _P, _P, _P]),
+    "sbr_trace_ray_list": (_I32, [_P, _P, _P, _P, _SZ, _P]),
     "sbr_run_noalloc": (_I32, [_P, _P, _P, _P, _P]),
     "sbr_adjoint": (_I32, [_P, _P, C.c_size_t, _P, _P, _P, _P]),
     "sbr_scene_update_vertices": (_I32, [_P, _P, _SZ]),

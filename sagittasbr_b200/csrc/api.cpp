@@ -235,13 +235,12 @@ sbr_status sbr_load_obj(const char* path, float** xyz, size_t* nverts, uint32_t*
             }
             if (face.size() < 3) continue;
             if (face.size() == 4) {
+                // squared diagonal lengths in FP32, summed x, y, z in order, as the
+                // loader computes them (real_t = float; near-square quads depend on it)
                 auto d2 = [&](int64_t a, int64_t c) {
-                    double s = 0;
-                    for (int q = 0; q < 3; ++q) {
-                        double d = double(V[3 * c + q]) - double(V[3 * a + q]);
-                        s += d * d;
-                    }
-                    return s;
+                    const float dx = V[3 * c] - V[3 * a], dy = V[3 * c + 1] - V[3 * a + 1],
+                                dz = V[3 * c + 2] - V[3 * a + 2];
+                    return dx * dx + dy * dy + dz * dz;
                 };
                 if (d2(face[0], face[2]) < d2(face[1], face[3])) {
                     uint32_t t6[6] = {(uint32_t)face[0], (uint32_t)face[1], (uint32_t)face[2],

@@ -663,4 +663,47 @@ sbr_status sbr_trace_records(sbr_scene* s, const sbr_job* job, const sbr_run_opt
     return st;
 }
 
+sbr_status sbr_trace_ray_list(sbr_scene* s, const sbr_job* job, const sbr_run_opts* opts, const int32_t* rays,
+                              size_t n_rays, sbr_ray_record* out) {
+    if (!s || !job || (n_rays && (!rays || !out))) return fail(SBR_ERR_INVALID_ARG, "null argument");
+    for (size_t k = 0; k < n_rays; ++k) {
+        const int32_t a = rays[3 * k], i = rays[3 * k + 1], j = rays[3 * k + 2];
+        if (a < 0 || a >= job->n_angles || i < 0 || i >= job->nx || j < 0 || j >= job->ny)
+            return fail(SBR_ERR_INVALID_ARG, "listed ray outside the job's angles or ray grid");
+    }
+    sbr_run_opts o{};
+    if (opts) o = *opts;
+    o.polarization = SBR_POL_SCALAR;
+    o.mode = SBR_MODE_BATCHED;
+    o.first_hit = SBR_FIRST_HIT_TRAVERSE;
+    sbr_plan* p = nullptr;
+    sbr_status st = sbr_plan_create(s, job, 1, &o, &p);
+    if (st != SBR_OK) return st;
+    int32_t* d_rays = nullptr;
+    sbr_ray_record* d = nullptr;
+    const size_t n = std::max<size_t>(n_rays, 1);
+    cudaError_t e = cudaMalloc(&d_rays, n * 3 * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&d, n * sizeof(sbr_ray_record));
+    if (e != cudaSuccess) st = fail(SBR_ERR_OOM, "ray list allocation failed");
+    if (st == SBR_OK && n_rays) {
+        e = cudaMemcpyAsync(d_rays, rays, n_rays * 3 * sizeof(int32_t), cudaMemcpyHostToDevice, p->stream);
+        if (e != cudaSuccess) st = cuda_fail(e, "ray list copy");
+    }
+    if (st == SBR_OK) st = fill_records(d, (long long)n_rays, p->stream);
+    if (st == SBR_OK) st = trace_list_launch(p, d_rays, (long long)n_rays, d);
+    if (st == SBR_OK) {
+        e = cudaStreamSynchronize(p->stream);
+        if (e != cudaSuccess) st = cuda_fail(e, "trace ray list");
+    }
+    if (st == SBR_OK) st = check_device_errors(p);
+    if (st == SBR_OK && n_rays) {
+        e = cudaMemcpy(out, d, n_rays * sizeof(sbr_ray_record), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) st = cuda_fail(e, "record copy");
+    }
+    cudaFree(d);
+    cudaFree(d_rays);
+    release(p);
+    return st;
+}
+
 }  // extern "C"

@@ -133,6 +133,8 @@ sbr_status build_tables(const sbr_scene* const* scenes, const int32_t* job_scene
 
 sbr_status plan_launch(sbr_plan* pl, bool records, sbr_ray_record* d_records);
 sbr_status fill_records(sbr_ray_record* d, long long n, cudaStream_t st);
+// Traces the listed rays (angle index, i, j; checked by the caller) of a one-job plan.
+sbr_status trace_list_launch(sbr_plan* pl, const int32_t* d_rays, long long n, sbr_ray_record* d_out);
 int max_freqs_per_job();
 sbr_status ensure_fp64(sbr_scene* s);
 sbr_status ensure_adjoint_data(sbr_scene* s);

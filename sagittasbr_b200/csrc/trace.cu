@@ -409,6 +409,55 @@ __global__ void __launch_bounds__(kCtaThreads, kMinCtasPerSm) k_trace(const Trac
     if (err) atomicOr(P.err, err);
 }
 
+// ------------------------------------------------------- listed rays (diagnostics)
+struct TraceListParams {
+    SceneView S;
+    const Segment* segs;
+    const JobConst* jobs;
+    const int32_t* rays;   // [n][3]: segment (angle of the plan's one job), i, j -- checked by the host
+    long long n;
+    uint32_t* err;
+    sbr_ray_record* out;   // [n]
+};
+
+// One thread per listed ray: the sweep kernel's own ray start, bounce step and
+// finish (ray.cuh), with the record written as k_trace writes it.
+template <int PREC>
+__global__ void __launch_bounds__(128) k_trace_list(const TraceListParams P) {
+    constexpr bool F64 = PREC == SBR_PREC_FP64;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= P.n) return;
+    const Segment& G = P.segs[P.rays[3 * t]];
+    const JobConst J = P.jobs[G.job];
+    const int i = P.rays[3 * t + 1], j = P.rays[3 * t + 2];
+    sbr_ray_record* rec = P.out + t;
+    uint32_t err = 0;
+    RayF rf;
+    RayD rd;
+    PolF ef;
+    PolD ed;
+    if (F64) start_d(rd, G, J, i, j);
+    else start_f<PREC>(rf, G, J, i, j);
+    if (J.max_bounces > 0) {
+        bool done = false;
+        while (!done)
+            done = F64 ? step_d<true, false>(rd, ed, P.S, J.max_bounces, err, rec)
+                       : step_f<PREC, true, false>(rf, ef, P.S, J.max_bounces, err, rec, nullptr);
+    }
+    const RayOut out = F64 ? finish_d(rd, J) : finish_f<PREC>(rf, J);
+    rec->count = F64 ? rd.count : rf.count;
+    rec->flags = 1;
+    rec->dist = out.L;
+    if (F64) {
+        rec->normal[0] = float(rd.nl.x); rec->normal[1] = float(rd.nl.y); rec->normal[2] = float(rd.nl.z);
+        rec->lastdir[0] = float(rd.dl.x); rec->lastdir[1] = float(rd.dl.y); rec->lastdir[2] = float(rd.dl.z);
+    } else {
+        rec->normal[0] = rf.nl.x; rec->normal[1] = rf.nl.y; rec->normal[2] = rf.nl.z;
+        rec->lastdir[0] = rf.dl.x; rec->lastdir[1] = rf.dl.y; rec->lastdir[2] = rf.dl.z;
+    }
+    if (err) atomicOr(P.err, err);
+}
+
 // ------------------------------------------------------- first-hit raster
 struct RasterParams {
     SceneView S;
@@ -705,6 +754,24 @@ sbr_status plan_launch(sbr_plan* pl, bool records, sbr_ray_record* d_records) {
     SBR_CUDA(cudaGetLastError());
     ++launches;
     pl->launches = launches;
+    return SBR_OK;
+}
+
+sbr_status trace_list_launch(sbr_plan* pl, const int32_t* d_rays, long long n, sbr_ray_record* d_out) {
+    if (n <= 0) return SBR_OK;
+    TraceListParams p{};
+    p.S = pl->scene_view;
+    p.segs = pl->d_segs;
+    p.jobs = pl->d_jobs;
+    p.rays = d_rays;
+    p.n = n;
+    p.err = pl->d_err;
+    p.out = d_out;
+    const void* fn = pl->prec == SBR_PREC_FP64   ? reinterpret_cast<const void*>(&k_trace_list<SBR_PREC_FP64>)
+                     : pl->prec == SBR_PREC_FP32 ? reinterpret_cast<const void*>(&k_trace_list<SBR_PREC_FP32>)
+                                                 : reinterpret_cast<const void*>(&k_trace_list<SBR_PREC_MIXED>);
+    void* args[] = {&p};
+    SBR_CUDA(cudaLaunchKernel(fn, dim3((unsigned)((n + 127) / 128)), dim3(128), args, 0, pl->stream));
     return SBR_OK;
 }
 

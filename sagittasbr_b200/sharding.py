@@ -89,6 +89,86 @@ def gather_samples(local_index: np.ndarray, local_values: np.ndarray, n_total: i
     return vals[order]
 
 
+def shard_of(scene, job, rank: int, world: int, balance: str = "cost") -> list[tuple[int, int]]:
+    """(start, count) of every rank's contiguous shard of `job`'s angles: the
+    reference's block rule, or balanced by the estimated rays of each angle."""
+    th = np.asarray(job.theta_deg, dtype=np.float64)
+    ph = np.asarray(job.phi_deg, dtype=np.float64)
+    if balance == "cost":
+        info = scene.info()
+        costs = aperture_cost(info["aabb_lo"], info["aabb_hi"], th, ph, job.nx, job.ny, job.grid_size)
+        return cost_partition(costs, world)
+    return [block_partition(th.size, world, r) for r in range(world)]
+
+
+class _DeviceArray:
+    """__cuda_array_interface__ view of a device pointer, so torch can wrap a plan's
+    result buffer without a copy."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, False), "version": 2,
+                                         "strides": None}
+
+
+class ShardedPlan:
+    """One sweep split over the ranks of a process group: this rank's contiguous
+    shard of the job's angles as a plan resident on its GPU, and a gather of every
+    rank's fields to rank 0 in global angle order straight from device memory
+    (all_gather of the padded FP64 field buffers: NCCL over NVLink between GPUs,
+    staged through host memory with gloo).  Replaces the reference's MPI partition
+    and MPI_Gatherv of results (src/app/sweep.cu:172-179, :465-526)."""
+
+    def __init__(self, scene, job, rank: int, world: int, balance: str = "cost", group=None, **plan_kw):
+        import sagittasbr_b200 as sbr
+        self.rank, self.world, self.group = rank, world, group
+        self.parts = shard_of(scene, job, rank, world, balance)
+        self.start, self.count = self.parts[rank]
+        self.n_freqs = job.n_freqs
+        self.n_angles = int(np.asarray(job.theta_deg).size)
+        self.max_count = max(c for _, c in self.parts)
+        self.plan = None
+        if self.count:
+            sl = slice(self.start, self.start + self.count)
+            sub = sbr.JobSpec(np.asarray(job.theta_deg, dtype=np.float64)[sl],
+                              np.asarray(job.phi_deg, dtype=np.float64)[sl], job.freqs_hz, job.nx, job.ny,
+                              job.grid_size, job.max_bounces, job.reflection_const)
+            self.plan = sbr.Plan(scene, [sub], **plan_kw)
+
+    def execute(self):
+        if self.plan is not None:
+            self.plan.execute()
+
+    def gather(self, torch):
+        """Every rank's field, on rank 0 as complex128 [n_angles, n_freqs] in angle
+        order (None elsewhere).  Collective: every rank calls it."""
+        import torch.distributed as dist
+        width = self.max_count * self.n_freqs * 2
+        dev = torch.device("cuda", torch.cuda.current_device())
+        buf = torch.zeros(width, dtype=torch.float64, device=dev)
+        if self.plan is not None:
+            # the plan may run on a stream of its own: let it finish before the copy
+            torch.cuda.synchronize()
+            ptr, _ = self.plan.device_results()
+            n = self.count * self.n_freqs * 2
+            buf[:n].copy_(torch.as_tensor(_DeviceArray(ptr, n), device=dev))
+        if dist.get_backend(self.group) == "gloo":
+            buf = buf.cpu()
+        parts = [torch.empty_like(buf) for _ in range(self.world)]
+        dist.all_gather(parts, buf, group=self.group)
+        if self.rank != 0:
+            return None
+        host = [p.cpu().numpy() for p in parts]
+        vals = np.concatenate([host[r][:c * self.n_freqs * 2] for r, (_, c) in enumerate(self.parts)])
+        if vals.size != self.n_angles * self.n_freqs * 2:
+            raise RuntimeError("gathered fields do not cover the sweep exactly once")
+        return (vals[0::2] + 1j * vals[1::2]).reshape(self.n_angles, self.n_freqs)
+
+    def close(self):
+        if self.plan is not None:
+            self.plan.close()
+            self.plan = None
+
+
 def sharded_sweep(scene, job, rank: int, world: int, balance: str = "cost", mode=None, precision=None):
     """Runs this rank's shard of `job`'s angles on its GPU and gathers every
     sample's complex field to rank 0 (returned there in angle order, else None)."""
@@ -96,12 +176,7 @@ def sharded_sweep(scene, job, rank: int, world: int, balance: str = "cost", mode
     th = np.asarray(job.theta_deg, dtype=np.float64)
     ph = np.asarray(job.phi_deg, dtype=np.float64)
     n = th.size
-    if balance == "cost":
-        info = scene.info()
-        costs = aperture_cost(info["aabb_lo"], info["aabb_hi"], th, ph, job.nx, job.ny, job.grid_size)
-        start, count = cost_partition(costs, world)[rank]
-    else:
-        start, count = block_partition(n, world, rank)
+    start, count = shard_of(scene, job, rank, world, balance)[rank]
     sl = slice(start, start + count)
     nf = job.n_freqs
     if count:

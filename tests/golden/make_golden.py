@@ -1,8 +1,8 @@
 """Generates the golden fixtures in tests/golden/ from the reference's OWN code.
 
-Run in a container where the reference tree is mounted (default /root/reference):
+Run where the reference tree is available, after `make -C oracle REF=<tree>`:
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py --ref <root of the reference tree>
 
 * ref_sbr.npz -- for every small case below: the field per (angle, frequency)
   and the per-ray hit records (hitCount, hitDist) of the reference's per-ray
@@ -67,7 +67,7 @@ def reference_mie(ref_root: str):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="root of the reference tree")
     a = ap.parse_args()
     O.build()
     if not O.ref_available(64):
