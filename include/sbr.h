@@ -290,13 +290,14 @@ sbr_status sbr_adjoint(sbr_scene* scene, const sbr_job* jobs, size_t n_jobs, con
  * SBR_ERR_UNSUPPORTED.
  * Set-up: the first call on a device looks up the device address of the array
  * (cudaGetSymbolAddress) with that device current; make that first call before
- * any stream capture.
+ * any stream capture.  The address is kept for the life of the process: a program
+ * that resets the device (cudaDeviceReset) must not call sbr_run_noalloc afterwards.
  * Sharing: every call on a device uses the same array, which keeps the previous
  * call's contents; each call clears the accumulators and queue it needs.  Calls
  * whose GPU work overlapped would race on the array and corrupt each other's
- * results, so the library serialises calls (one lock per process) and each call
- * returns only after its stream has finished; it then returns the device error
- * status. */
+ * results, so the library serialises calls (one lock per process) and each call,
+ * on success and on error alike, returns only after its stream has finished the
+ * work it queued; on success it returns the device error status. */
 #define SBR_NOALLOC_MAX_ANGLES 1024
 #define SBR_NOALLOC_MAX_SAMPLES 4096
 #define SBR_NOALLOC_SCRATCH_BYTES (448u * 1024u)

@@ -260,6 +260,7 @@ struct AdjointBuffers {
 // Caller vertices and triangles on the device (uploaded once per scene).
 sbr_status ensure_adjoint_data(sbr_scene* s) {
     if (s->d_xyz && s->d_idx) return SBR_OK;
+    sbr::DeviceGuard device_guard;
     SBR_CUDA(cudaSetDevice(s->device));
     const size_t vb = s->xyz.size() * sizeof(float), ib = s->idx.size() * sizeof(uint32_t);
     if (cudaMalloc(&s->d_xyz, vb) != cudaSuccess || cudaMalloc(&s->d_idx, ib) != cudaSuccess)

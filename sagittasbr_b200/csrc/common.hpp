@@ -22,6 +22,23 @@ sbr_status cuda_fail(cudaError_t e, const char* what);
         if (e__ != cudaSuccess) return sbr::cuda_fail(e__, #call); \
     } while (0)
 
+// Makes an entry point leave the caller's current device as it found it: records
+// the current device on construction and sets it back on every return path.
+class DeviceGuard {
+  public:
+    DeviceGuard() {
+        if (cudaGetDevice(&prev_) != cudaSuccess) prev_ = -1;
+    }
+    ~DeviceGuard() {
+        if (prev_ >= 0) cudaSetDevice(prev_);
+    }
+    DeviceGuard(const DeviceGuard&) = delete;
+    DeviceGuard& operator=(const DeviceGuard&) = delete;
+
+  private:
+    int prev_ = -1;
+};
+
 // Device-side error word bits (written by kernels, read after each execute).
 enum : uint32_t {
     DEV_ERR_STACK = 1u,      // traversal stack would overflow (entry dropped)

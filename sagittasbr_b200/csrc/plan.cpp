@@ -79,6 +79,7 @@ sbr_status zalloc(T** d, size_t count, int64_t& bytes) {
 
 void release(sbr_plan* p) {
     if (!p) return;
+    sbr::DeviceGuard device_guard;
     cudaSetDevice(p->scene->device);
     if (p->stream) cudaStreamSynchronize(p->stream);
     if (p->graph) cudaGraphExecDestroy(p->graph);
@@ -384,6 +385,7 @@ sbr_status plan_create(sbr_scene* const* scenes, size_t n_scenes, const int32_t*
         for (size_t j = 0; j < n_jobs; ++j)
             if (job_scene[j] < 0 || (size_t)job_scene[j] >= n_scenes)
                 return fail(SBR_ERR_INVALID_ARG, "job scene index out of range");
+    sbr::DeviceGuard device_guard;
     SBR_CUDA(cudaSetDevice(s->device));
     if (o.precision == SBR_PREC_FP64) {
         for (size_t k = 0; k < n_scenes; ++k) {
@@ -525,6 +527,7 @@ sbr_status sbr_plan_create_multi(sbr_scene* const* scenes, size_t n_scenes, cons
 
 sbr_status sbr_plan_execute(sbr_plan* p) {
     if (!p) return fail(SBR_ERR_INVALID_ARG, "plan is null");
+    sbr::DeviceGuard device_guard;
     SBR_CUDA(cudaSetDevice(p->scene->device));
     SBR_CUDA(cudaEventRecord(p->ev0, p->stream));
     if (p->use_graph && p->mode == SBR_MODE_BATCHED) {
@@ -553,6 +556,7 @@ sbr_status sbr_plan_execute(sbr_plan* p) {
 sbr_status sbr_plan_results(sbr_plan* p, sbr_result* out) {
     if (!p || !out) return fail(SBR_ERR_INVALID_ARG, "null argument");
     if (!p->executed) return fail(SBR_ERR_INVALID_ARG, "plan was not executed");
+    sbr::DeviceGuard device_guard;
     SBR_CUDA(cudaSetDevice(p->scene->device));
     SBR_CUDA(cudaEventSynchronize(p->ev1));
     sbr_status st = check_device_errors(p);
@@ -633,6 +637,8 @@ sbr_status sbr_run(sbr_scene* s, const sbr_job* jobs, size_t n_jobs, sbr_result*
 
 sbr_status sbr_trace_records(sbr_scene* s, const sbr_job* job, const sbr_run_opts* opts, sbr_ray_record* out) {
     if (!s || !job || !out) return fail(SBR_ERR_INVALID_ARG, "null argument");
+    sbr::DeviceGuard device_guard;
+    SBR_CUDA(cudaSetDevice(s->device));
     // hit records do not depend on the polarisation: trace them with the scalar plan
     sbr_run_opts o{};
     if (opts) o = *opts;
@@ -671,6 +677,8 @@ sbr_status sbr_trace_ray_list(sbr_scene* s, const sbr_job* job, const sbr_run_op
         if (a < 0 || a >= job->n_angles || i < 0 || i >= job->nx || j < 0 || j >= job->ny)
             return fail(SBR_ERR_INVALID_ARG, "listed ray outside the job's angles or ray grid");
     }
+    sbr::DeviceGuard device_guard;
+    SBR_CUDA(cudaSetDevice(s->device));
     sbr_run_opts o{};
     if (opts) o = *opts;
     o.polarization = SBR_POL_SCALAR;

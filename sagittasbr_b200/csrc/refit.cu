@@ -134,6 +134,7 @@ extern "C" sbr_status sbr_scene_update_vertices(sbr_scene* s, const float* xyz, 
     if (nverts * 3 != s->xyz.size()) return fail(SBR_ERR_INVALID_ARG, "vertex count differs from the scene's");
     for (size_t i = 0; i < 3 * nverts; ++i)
         if (!std::isfinite(xyz[i])) return fail(SBR_ERR_NONFINITE, "non-finite vertex coordinate");
+    sbr::DeviceGuard device_guard;
     SBR_CUDA(cudaSetDevice(s->device));
     sbr_status st = ensure_adjoint_data(s);  // device copies of the caller's vertices and triangles
     if (st != SBR_OK) return st;

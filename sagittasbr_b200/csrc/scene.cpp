@@ -102,6 +102,7 @@ sbr_status ensure_fp64(sbr_scene* s) {
         if (len > 0) { g.n[0] = nx / len; g.n[1] = ny / len; g.n[2] = nz / len; }
         else { g.n[0] = g.n[1] = g.n[2] = 0.0; }
     }
+    sbr::DeviceGuard device_guard;
     SBR_CUDA(cudaSetDevice(s->device));
     size_t bytes = sizeof(GTri64) * t64.size();
     cudaError_t e = cudaMalloc(&s->d_tris64, bytes);
@@ -139,6 +140,7 @@ sbr_status sbr_scene_create(const float* xyz, size_t nverts, const uint32_t* tri
     cudaDeviceProp prop;
     SBR_CUDA(cudaGetDeviceProperties(&prop, dev));
     if (prop.major < 10) return fail(SBR_ERR_NO_DEVICE, "libsbr is built for sm_100a (B200); device is older");
+    sbr::DeviceGuard device_guard;
     SBR_CUDA(cudaSetDevice(dev));
 
     auto t0 = std::chrono::steady_clock::now();
@@ -372,6 +374,7 @@ sbr_status sbr_scene_info_get(const sbr_scene* s, sbr_scene_info* out) {
 
 sbr_status sbr_scene_cancel(sbr_scene* s) {
     if (!s) return fail(SBR_ERR_INVALID_ARG, "scene is null");
+    sbr::DeviceGuard device_guard;
     SBR_CUDA(cudaSetDevice(s->device));
     SBR_CUDA(cudaMemcpyAsync(s->d_cancel, &s->h_flag_vals[0], sizeof(int32_t), cudaMemcpyHostToDevice,
                              s->cancel_stream));
@@ -380,6 +383,7 @@ sbr_status sbr_scene_cancel(sbr_scene* s) {
 
 sbr_status sbr_scene_reset_cancel(sbr_scene* s) {
     if (!s) return fail(SBR_ERR_INVALID_ARG, "scene is null");
+    sbr::DeviceGuard device_guard;
     SBR_CUDA(cudaSetDevice(s->device));
     SBR_CUDA(cudaMemcpyAsync(s->d_cancel, &s->h_flag_vals[1], sizeof(int32_t), cudaMemcpyHostToDevice,
                              s->cancel_stream));

@@ -313,7 +313,7 @@ __global__ void __launch_bounds__(kCtaThreads, kMinCtasPerSm) k_trace(const Trac
                     }
                 }
             }
-            if (!TRANSPOSED) {
+            if constexpr (!TRANSPOSED) {
                 if (done && out.amp != 0.0f) {
 #pragma unroll
                     for (int ch = 0; ch < NACC; ++ch) {
@@ -365,7 +365,7 @@ __global__ void __launch_bounds__(kCtaThreads, kMinCtasPerSm) k_trace(const Trac
         // ---- fold the item: lanes -> warp in a fixed order, then fixed point.
         // Channel ch of sample (sbase + k) lives at accumulator (sbase * NPOL + ch).
         const long long cbase = (G.sample_base + kb) * NPOL;
-        if (!TRANSPOSED) {
+        if constexpr (!TRANSPOSED) {
 #pragma unroll
             for (int ch = 0; ch < NACC; ++ch) {
                 if (ch < KC) {
@@ -390,8 +390,13 @@ __global__ void __launch_bounds__(kCtaThreads, kMinCtasPerSm) k_trace(const Trac
                 if (ch < KC) {
                     const double invQ = fold_factor<PREC>(F[POL ? ch >> 1 : ch]);
                     unsigned long long* A = P.acc + 2 * ((cbase + ch) * P.n_rep + rep);
-                    add_fixed(A, SACC ? my_acc[c * 32].x : accRe[c], invQ);
-                    add_fixed(A + 1, SACC ? my_acc[c * 32].y : accIm[c], invQ);
+                    if constexpr (SACC) {
+                        add_fixed(A, my_acc[c * 32].x, invQ);
+                        add_fixed(A + 1, my_acc[c * 32].y, invQ);
+                    } else {
+                        add_fixed(A, accRe[c], invQ);
+                        add_fixed(A + 1, accIm[c], invQ);
+                    }
                 }
             }
         }
@@ -886,6 +891,7 @@ extern "C" sbr_status sbr_run_noalloc(sbr_scene* s, const sbr_job* job, double* 
         return fail(SBR_ERR_UNSUPPORTED, "allocation-free FP64 sweep needs a scene created with want_fp64 = 1");
 
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    sbr::DeviceGuard device_guard;
     SBR_CUDA(cudaSetDevice(s->device));
     NoallocScratch* D = nullptr;
     st = noalloc_address(s->device, &D);
@@ -899,6 +905,12 @@ extern "C" sbr_status sbr_run_noalloc(sbr_scene* s, const sbr_job* job, double* 
     if (st != SBR_OK) return st;
 
     cudaStream_t stream = o.stream ? (cudaStream_t)o.stream : s->stream;
+    // From the first queued copy on, every return waits for this call's work on the
+    // shared array, so the next call (after the lock is released) cannot overlap it.
+    struct StreamDrain {
+        cudaStream_t st;
+        ~StreamDrain() { cudaStreamSynchronize(st); }
+    } drain{stream};
     const size_t nseg = (size_t)sink.n_segs, nsamp = (size_t)sink.n_samples;
     // tables in; accumulators, counters and queue head cleared (the array keeps the last call's contents)
     SBR_CUDA(cudaMemcpyAsync(D->tables.segs, g_noalloc_host.segs, nseg * sizeof(Segment), cudaMemcpyHostToDevice,

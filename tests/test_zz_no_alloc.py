@@ -9,7 +9,8 @@ output arrays (here two torch tensors, allocated by the test, not by the call).
 The test calls it twice in a row through the C ABI and checks both results
 against the allocating entry point sbr_run, with the tolerance of the other GPU
 tests for identical arithmetic (the two paths build the same tables and run the
-same kernels, so the fields agree to rounding of the final conversion).  It also
+same kernels, so the fields agree to rounding of the final conversion), and that
+the device's free memory is the same before and after the second call.  It also
 checks the size limit.  This file sorts last so a failure here stops a `-x` run
 only after every other test has run; it passes alone as well.
 """
@@ -45,8 +46,15 @@ def test_noalloc_matches_allocating_run_on_two_calls():
         field = torch.full((2 * len(th) * len(fr),), -1.0, dtype=torch.float64, device="cuda")
         stats = torch.full((4 * len(th),), -1, dtype=torch.int64, device="cuda")
         torch.cuda.synchronize()
+        free_before = None
         for call in range(2):
+            if call == 1:
+                # the first call may load the module; from then on nothing is allocated
+                torch.cuda.synchronize()
+                free_before = torch.cuda.mem_get_info()[0]
             _lib.check(_call(scene, job_c, field, stats, opts), "sbr_run_noalloc")
+            if call == 1:
+                assert torch.cuda.mem_get_info()[0] == free_before, "device memory changed across the call"
             f = field.cpu().numpy()
             got = f[0::2] + 1j * f[1::2]
             np.testing.assert_allclose(got, ref.field, rtol=1e-12, atol=1e-14 * np.abs(ref.field).max())
