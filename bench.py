@@ -598,6 +598,8 @@ def main():
     ap.add_argument("--polarization", default="scalar", choices=["scalar", "hhvv"],
                     help="the reference's scalar PO term, or HH and VV fields with E-vector tracking")
     ap.add_argument("--gpu-build", action="store_true", help="build the scene's SAH tree on the GPU")
+    ap.add_argument("--node-width", type=int, default=4, choices=[4, 8],
+                    help="BVH node width walked by the sweep kernel (8: the opt-in 8-wide tree)")
     ap.add_argument("--no-ref-gpu", action="store_true",
                     help="skip the reference's own GPU build (baseline/_ref) on the same GPU")
     ap.add_argument("--fp64-check", type=int, default=16,
@@ -634,7 +636,7 @@ def main():
     torch.cuda.set_stream(stream)
     sp = stream.cuda_stream
     t_scene = time.perf_counter()
-    scene = sbr.Scene(w["verts"], w["tris"], device=local, gpu_build=args.gpu_build)
+    scene = sbr.Scene(w["verts"], w["tris"], device=local, gpu_build=args.gpu_build, node_width=args.node_width)
     scene_s = time.perf_counter() - t_scene
     sah_ms = scene.info()["sah_ms"]
     job = sbr.JobSpec(w["theta"], w["phi"], w["freqs"], w["nx"], w["ny"], w["G"], w["max_bounces"], w["R"])
@@ -784,7 +786,7 @@ def main():
                 "parallelism": (f"{ws} GPUs, cost-balanced angle shards of one sweep, fields gathered to rank 0 "
                                 "inside the timed region") if ws > 1 else "1 GPU",
                 "scene_build_s": scene_s, "sah_build": {"where": "gpu" if args.gpu_build else "host", "ms": sah_ms},
-                "plan_s": plan_s, "autotune": bool(args.autotune),
+                "plan_s": plan_s, "autotune": bool(args.autotune), "node_width": args.node_width,
                 "blocks_per_item": info["blocks_per_item"], "ctas_per_sm": info["ctas_per_sm"]},
         "mray_bounces_per_s": bounces_all / (step_ms * 1e-3) / 1e6,
         "closest_hit_queries_per_s": queries_all / (step_ms * 1e-3),

@@ -64,7 +64,10 @@ typedef struct sbr_build_opts {
     int32_t want_fp64;    /* also upload FP64 triangles (needed by SBR_PREC_FP64); -1 -> lazily */
     int32_t gpu_build;    /* 1: build the binary SAH tree on the GPU (same tree as the host build;
                              triangles inside a leaf may be ordered differently) */
-    int32_t reserved[2];
+    int32_t node_width;   /* 0 or 4: 4-wide nodes (default); 8: the mixed-precision scalar sweep
+                             walks 8-wide nodes built over the same leaves (the other kernels keep
+                             the 4-wide tree; the same closest hits either way) */
+    int32_t reserved[1];
 } sbr_build_opts;
 
 typedef struct sbr_scene_info {
@@ -99,7 +102,8 @@ sbr_status sbr_scene_reset_cancel(sbr_scene* scene);
  * gradient step moves the vertices a little (traversal slows down as the
  * deformation grows; create a new scene then).  Plans created before the update
  * keep their launcher tables (aperture clipping, launch-plane placement): create
- * plans after it.  No counterpart in the reference. */
+ * plans after it.  An opt-in 8-wide tree (node_width 8) is released, not refitted.
+ * No counterpart in the reference. */
 sbr_status sbr_scene_update_vertices(sbr_scene* scene, const float* xyz, size_t nverts);
 
 /* --------------------------------------------------------------------- job */

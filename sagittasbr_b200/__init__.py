@@ -44,7 +44,8 @@ class Scene:
     """Triangle mesh resident on one GPU with its BVH (sbr_scene_create)."""
 
     def __init__(self, verts, tris, model_scale: float = 1.0, device: int = -1, leaf_size: int = 0,
-                 bin_count: int = 0, n_threads: int = 0, want_fp64: bool = False, gpu_build: bool = False):
+                 bin_count: int = 0, n_threads: int = 0, want_fp64: bool = False, gpu_build: bool = False,
+                 node_width: int = 0):
         v = np.ascontiguousarray(verts, dtype=np.float32).reshape(-1, 3)
         t = np.ascontiguousarray(tris, dtype=np.uint32).reshape(-1, 3)
         o = _lib.BuildOpts()
@@ -55,6 +56,7 @@ class Scene:
         o.n_threads = int(n_threads)
         o.want_fp64 = 1 if want_fp64 else 0
         o.gpu_build = 1 if gpu_build else 0
+        o.node_width = int(node_width)
         h = C.c_void_p()
         check(lib().sbr_scene_create(_p(v), v.shape[0], _p(t), t.shape[0], C.byref(o), C.byref(h)),
               "sbr_scene_create")

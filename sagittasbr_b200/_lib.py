@@ -30,7 +30,8 @@ class BuildOpts(C.Structure):
         ("n_threads", C.c_int32),
         ("want_fp64", C.c_int32),
         ("gpu_build", C.c_int32),
-        ("reserved", C.c_int32 * 2),
+        ("node_width", C.c_int32),
+        ("reserved", C.c_int32 * 1),
     ]
 
 

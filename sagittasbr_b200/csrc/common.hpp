@@ -58,6 +58,14 @@ struct __align__(16) GNode4 {
 };
 static_assert(sizeof(GNode4) == 112, "GNode4 must be 112 bytes");
 
+// 8-wide node (opt-in, sbr_build_opts.node_width = 8): two 4-wide halves holding
+// children 0-3 and 4-7, fourteen 16 B loads.  Inner child references index the
+// 8-wide node array; leaves and empty slots are encoded as in GNode4.
+struct __align__(16) GNode8 {
+    GNode4 q[2];
+};
+static_assert(sizeof(GNode8) == 224, "GNode8 must be 224 bytes");
+
 constexpr int kLeafMax = 15;
 constexpr int kStackDepth = 64;     // reference uses 64 (src/cuda/rtKernels.cu:65)
 
@@ -82,6 +90,7 @@ struct SceneView {
     const GTri* __restrict__ tris;
     const GTri64* __restrict__ tris64;
     const int32_t* __restrict__ tri_id;
+    const GNode8* __restrict__ nodes8;  // the 8-wide tree of the same leaves, or null
 };
 
 // --------------------------------------------------------------- plan data

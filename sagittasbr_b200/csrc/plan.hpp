@@ -22,6 +22,8 @@ struct sbr_scene {
     // device
     sbr::GNode4* d_nodes = nullptr;
     int64_t n_gnodes = 0;
+    sbr::GNode8* d_nodes8 = nullptr;  // node_width 8: the same leaves under 8-wide nodes
+    int64_t n_gnodes8 = 0;
     int64_t n_bin_nodes = 0;
     sbr::GTri* d_tris = nullptr;
     sbr::GTri64* d_tris64 = nullptr;
@@ -43,7 +45,7 @@ struct sbr_scene {
     float* d_tri_box = nullptr;
     int64_t device_bytes = 0;
 
-    sbr::SceneView view() const { return sbr::SceneView{d_nodes, d_tris, d_tris64, d_tri_id}; }
+    sbr::SceneView view() const { return sbr::SceneView{d_nodes, d_tris, d_tris64, d_tri_id, d_nodes8}; }
 };
 
 struct sbr_plan {

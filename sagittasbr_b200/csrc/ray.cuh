@@ -99,7 +99,7 @@ __device__ __forceinline__ void start_f(RayF& r, const Segment& G, const JobCons
 // One closest-hit query, then reflect and nudge; true when the ray is finished.
 // The first query is read from the first-hit buffer when there is one (and the
 // entry is restored to empty for the next chunk).
-template <int PREC, bool REC, bool POL>
+template <int PREC, bool REC, bool POL, bool W8 = false>
 __device__ __forceinline__ bool step_f(RayF& r, PolF& e, const SceneView& S, int maxB, uint32_t& err,
                                        sbr_ray_record* rec, unsigned long long* zbuf) {
     float tB = 1e20f;
@@ -110,6 +110,9 @@ __device__ __forceinline__ bool step_f(RayF& r, PolF& e, const SceneView& S, int
         if (key == ~0ull) return true;
         tB = __uint_as_float((unsigned)(key >> 32));
         slot = (int)(unsigned)key;
+    } else if constexpr (W8) {
+        static_assert(PREC == SBR_PREC_MIXED && !REC && !POL, "the 8-wide walk is the mixed scalar sweep's");
+        slot = Walker8::closest(S, r.o, r.d, 1.0e-3f, tB, err);
     } else {
         slot = Walker<false>::closest<PREC == SBR_PREC_MIXED, !REC && !POL>(S, r.o, r.d, 1.0e-3f, tB, err);
     }

@@ -138,6 +138,12 @@ extern "C" sbr_status sbr_scene_update_vertices(sbr_scene* s, const float* xyz, 
     SBR_CUDA(cudaSetDevice(s->device));
     sbr_status st = ensure_adjoint_data(s);  // device copies of the caller's vertices and triangles
     if (st != SBR_OK) return st;
+    if (s->d_nodes8) {  // the opt-in 8-wide tree is not refitted: the sweep walks the 4-wide one again
+        SBR_CUDA(cudaStreamSynchronize(s->stream));
+        cudaFree(s->d_nodes8);
+        s->d_nodes8 = nullptr;
+        s->n_gnodes8 = 0;
+    }
     if (!s->d_refit_nodes) {
         const size_t nb = s->refit_nodes.size() * sizeof(int32_t), bb = 6 * (size_t)s->ntris * sizeof(float);
         if (cudaMalloc(&s->d_refit_nodes, nb) != cudaSuccess || cudaMalloc(&s->d_tri_box, bb) != cudaSuccess)

@@ -64,6 +64,7 @@ void free_scene(sbr_scene* s) {
     cudaSetDevice(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
     cudaFree(s->d_nodes);
+    cudaFree(s->d_nodes8);
     cudaFree(s->d_tris);
     cudaFree(s->d_tris64);
     cudaFree(s->d_tri_id);
@@ -127,6 +128,8 @@ sbr_status sbr_scene_create(const float* xyz, size_t nverts, const uint32_t* tri
     if (opts) o = *opts;
     double scale = o.model_scale == 0.0 ? 1.0 : o.model_scale;
     if (!std::isfinite(scale)) return fail(SBR_ERR_NONFINITE, "model scale is not finite");
+    if (o.node_width != 0 && o.node_width != 4 && o.node_width != 8)
+        return fail(SBR_ERR_INVALID_ARG, "node_width must be 0, 4 or 8");
     for (size_t i = 0; i < 3 * ntris; ++i)
         if (tri_idx[i] >= nverts) return fail(SBR_ERR_BAD_INDEX, "triangle index out of range");
     for (size_t i = 0; i < 3 * nverts; ++i)
@@ -278,6 +281,66 @@ sbr_status sbr_scene_create(const float* xyz, size_t nverts, const uint32_t* tri
         }
     }
     s->n_gnodes = (int64_t)g.size();
+
+    // Opt-in 8-wide tree over the same leaves: the same greedy collapse, opening
+    // the largest inner child until a node holds eight children (or the walker's
+    // stack bound is reached).
+    std::vector<GNode8> g8;
+    if (o.node_width == 8) {
+        auto fill8 = [&](GNode8& n, int c, const BinNode* b, int ref) { fill(n.q[c >> 2], c & 3, b, ref); };
+        if (tree.nodes[0].left < 0) {
+            GNode8 n;
+            fill8(n, 0, &tree.nodes[0], leafRef(tree.nodes[0]));
+            for (int c = 1; c < 8; ++c) fill8(n, c, nullptr, ~0);
+            g8.push_back(n);
+        } else {
+            struct Work8 {
+                int32_t bin, slot, need;
+            };
+            g8.reserve(tree.nodes.size() / 4 + 1);
+            g8.emplace_back();
+            std::vector<Work8> work{{0, 0, 0}};
+            while (!work.empty()) {
+                const Work8 w = work.back();
+                work.pop_back();
+                int32_t kids[8] = {tree.nodes[w.bin].left, tree.nodes[w.bin].right, -1, -1, -1, -1, -1, -1};
+                int nk = 2;
+                while (nk < 8 && w.need + nk <= kStackDepth) {
+                    int best = -1;
+                    float ba = -1.0f;
+                    for (int k = 0; k < nk; ++k) {
+                        const BinNode& K = tree.nodes[kids[k]];
+                        if (K.left >= 0 && area(K) > ba) { ba = area(K); best = k; }
+                    }
+                    if (best < 0) break;
+                    const BinNode& K = tree.nodes[kids[best]];
+                    for (int k = nk; k > best + 1; --k) kids[k] = kids[k - 1];
+                    kids[best] = K.left;
+                    kids[best + 1] = K.right;
+                    ++nk;
+                }
+                GNode8 n;
+                Work8 inner[8];
+                int ni = 0;
+                const int32_t need = w.need + nk - 1;
+                for (int c = 0; c < 8; ++c) {
+                    if (c >= nk) { fill8(n, c, nullptr, ~0); continue; }
+                    const BinNode& K = tree.nodes[kids[c]];
+                    if (K.left >= 0) {
+                        const int32_t idx = (int32_t)g8.size() + ni;
+                        inner[ni++] = {kids[c], idx, need};
+                        fill8(n, c, &K, idx);
+                    } else {
+                        fill8(n, c, &K, leafRef(K));
+                    }
+                }
+                g8[w.slot] = n;
+                g8.resize(g8.size() + ni);
+                for (int q = ni - 1; q >= 0; --q) work.push_back(inner[q]);
+            }
+        }
+    }
+    s->n_gnodes8 = (int64_t)g8.size();
     // nodes grouped by depth (a refit recomputes the boxes deepest level first)
     {
         const int32_t maxd = *std::max_element(level.begin(), level.end());
@@ -344,6 +407,14 @@ sbr_status sbr_scene_create(const float* xyz, size_t nverts, const uint32_t* tri
         (e = cudaStreamCreateWithFlags(&s->cancel_stream, cudaStreamNonBlocking)) != cudaSuccess)
         return bail(cuda_fail(e, "cudaStreamCreate"));
     s->device_bytes = (int64_t)(nb + tb + ib);
+    if (!g8.empty()) {
+        const size_t nb8 = sizeof(GNode8) * g8.size();
+        if ((e = cudaMalloc(&s->d_nodes8, nb8)) != cudaSuccess)
+            return bail(fail(SBR_ERR_OOM, std::string("device allocation failed: ") + cudaGetErrorString(e)));
+        if ((e = cudaMemcpy(s->d_nodes8, g8.data(), nb8, cudaMemcpyHostToDevice)) != cudaSuccess)
+            return bail(cuda_fail(e, "8-wide node upload"));
+        s->device_bytes += (int64_t)nb8;
+    }
     if (o.want_fp64 > 0) {
         sbr_status st = ensure_fp64(s);
         if (st != SBR_OK) return bail(st);

@@ -185,7 +185,7 @@ __device__ __forceinline__ void add_fixed(unsigned long long* acc, double v, dou
 // the warp reduces them in a fixed order and adds the total, as int64 fixed
 // point, to one of the segment's accumulator replicas.  Which lane takes which
 // ray depends only on the item, so every sum is reproducible bit for bit.
-template <int PREC, int EPI, bool REC, bool POL, bool MULTI>
+template <int PREC, int EPI, bool REC, bool POL, bool MULTI, bool W8 = false>
 __global__ void __launch_bounds__(kCtaThreads, kMinCtasPerSm) k_trace(const TraceParams P) {
     constexpr unsigned FULL = 0xffffffffu;
     constexpr bool F64 = PREC == SBR_PREC_FP64;
@@ -286,7 +286,7 @@ __global__ void __launch_bounds__(kCtaThreads, kMinCtasPerSm) k_trace(const Trac
             out.amp = 0.0f;
             if (active) {
                 done = F64 ? step_d<REC, POL>(rd, ed, S, J.max_bounces, err, rec)
-                           : step_f<PREC, REC, POL>(rf, ef, S, J.max_bounces, err, rec, P.zbuf);
+                           : step_f<PREC, REC, POL, W8>(rf, ef, S, J.max_bounces, err, rec, P.zbuf);
                 ++queries;
                 if (done) {
                     const int cnt = F64 ? rd.count : rf.count;
@@ -590,9 +590,9 @@ __global__ void k_fill_records(sbr_ray_record* r, long long n) {
 // --------------------------------------------------------------------- host
 namespace {
 
-template <int PREC, int EPI, bool REC, bool POL, bool MULTI>
+template <int PREC, int EPI, bool REC, bool POL, bool MULTI, bool W8 = false>
 const void* kernel_ptr() {
-    return reinterpret_cast<const void*>(&k_trace<PREC, EPI, REC, POL, MULTI>);
+    return reinterpret_cast<const void*>(&k_trace<PREC, EPI, REC, POL, MULTI, W8>);
 }
 
 template <int PREC, bool REC, bool POL, bool MULTI = false>
@@ -610,8 +610,16 @@ const void* pick_epi_kernel(int epi) {
 // whether jobs trace different scenes.  Record kernels come with the two general
 // layouts only and one scene; polarised kernels in MIXED and FP64 precision only
 // (the host rejects the other combinations).
-const void* pick_kernel(int prec, int channels, bool rec, bool pol, bool multi = false) {
+const void* pick_kernel(int prec, int channels, bool rec, bool pol, bool multi = false, bool w8 = false) {
     int epi = pick_epi(channels);
+    if (w8 && prec == SBR_PREC_MIXED && !rec && !pol && !multi) {
+        switch (epi) {
+            case EPI_LANE1: return kernel_ptr<SBR_PREC_MIXED, EPI_LANE1, false, false, false, true>();
+            case EPI_LANE4: return kernel_ptr<SBR_PREC_MIXED, EPI_LANE4, false, false, false, true>();
+            case EPI_T64: return kernel_ptr<SBR_PREC_MIXED, EPI_T64, false, false, false, true>();
+            default: return kernel_ptr<SBR_PREC_MIXED, EPI_T128, false, false, false, true>();
+        }
+    }
     if (multi && !rec) {
         if (pol) return prec == SBR_PREC_FP64 ? pick_epi_kernel<SBR_PREC_FP64, false, true, true>(epi)
                                               : pick_epi_kernel<SBR_PREC_MIXED, false, true, true>(epi);
@@ -665,7 +673,8 @@ sbr_status plan_launch(sbr_plan* pl, bool records, sbr_ray_record* d_records) {
     const bool pol = pl->pol == SBR_POL_HHVV && !records;
     const int npol = pol ? 2 : 1;
     const bool batched = pl->mode == SBR_MODE_BATCHED || records;
-    const void* fn = pick_kernel(pl->prec, (batched ? pl->k_max : 1) * npol, records, pol, pl->multi);
+    const void* fn = pick_kernel(pl->prec, (batched ? pl->k_max : 1) * npol, records, pol, pl->multi,
+                                 pl->scene_view.nodes8 != nullptr);
     TraceParams p{};
     p.segpol = pl->d_segpol;
     p.scenes = pl->d_scenes;

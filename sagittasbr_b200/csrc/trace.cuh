@@ -451,6 +451,109 @@ struct Walker<false> {
     }
 };
 
+// Closest hit over the opt-in 8-wide tree (SceneView::nodes8), mixed precision:
+// the watertight triangle test and the two-wide slab planes of the 4-wide walker,
+// on both halves of a node.  One accepted child is entered directly; two or more
+// are ordered by entry distance (each half sorted, then an odd-even merge: 19
+// compare-exchanges), the nearest entered and the rest pushed farthest first.
+struct Walker8 {
+    __device__ __forceinline__ static int closest(const SceneView& S, F3 o, F3 d, float tMin, float& tBest,
+                                                  uint32_t& err) {
+        const F3 inv{slab_inv(d.x), slab_inv(d.y), slab_inv(d.z)};
+        const WtRay wr = wt_ray(d);
+        const F3 oi{o.x * inv.x, o.y * inv.y, o.z * inv.z};
+        const Slab2 R2 = slab2(inv, oi);
+        const unsigned onx = inv.x < 0.0f ? 16u : 0u, ony = inv.y < 0.0f ? 48u : 32u, onz = inv.z < 0.0f ? 80u : 64u;
+        const unsigned ofx = onx ^ 16u, ofy = ony ^ 16u, ofz = onz ^ 16u;
+        unsigned long long stack[kStackDepth];
+        int sp = 0;
+        int ref = 0;
+        int best = -1;
+        uint32_t iters = 0;
+        auto plane = [](const GNode4* p, unsigned off) {
+            return __ldg(reinterpret_cast<const float4*>(reinterpret_cast<const char*>(p) + off));
+        };
+        auto push = [&](int r, float t) {
+            if (sp < kStackDepth) stack[sp++] = pack_entry(r, t);
+            else err |= DEV_ERR_STACK;
+        };
+        auto pop = [&]() {
+            while (sp > 0) {
+                const unsigned long long e = stack[--sp];
+                if (__uint_as_float((unsigned)(e >> 32)) <= tBest) { ref = (int)(unsigned)e; return true; }
+            }
+            return false;
+        };
+        for (;;) {
+            while (ref >= 0) {
+                if (++iters > kIterBudget) { err |= DEV_ERR_BUDGET; return -1; }
+                const GNode4* np = S.nodes8[ref].q;
+                float t[8];
+                bool hh[8];
+                int c[8];
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const GNode4* q = np + h;
+                    const float4 nx = plane(q, onx), fx = plane(q, ofx), ny = plane(q, ony), fy = plane(q, ofy);
+                    const float4 nz = plane(q, onz), fz = plane(q, ofz);
+                    const int4 ch = __ldg(&q->child);
+                    float th[4];
+                    bool hk[4];
+                    slab4_nh(nx, fx, ny, fy, nz, fz, R2, tMin, tBest, th, hk);
+                    t[4 * h] = th[0]; t[4 * h + 1] = th[1]; t[4 * h + 2] = th[2]; t[4 * h + 3] = th[3];
+                    hh[4 * h] = hk[0]; hh[4 * h + 1] = hk[1]; hh[4 * h + 2] = hk[2]; hh[4 * h + 3] = hk[3];
+                    c[4 * h] = ch.x; c[4 * h + 1] = ch.y; c[4 * h + 2] = ch.z; c[4 * h + 3] = ch.w;
+                }
+                int nh = 0;
+#pragma unroll
+                for (int k = 0; k < 8; ++k) nh += int(hh[k]);
+                if (nh == 1) {
+#pragma unroll
+                    for (int k = 0; k < 8; ++k)
+                        if (hh[k]) ref = c[k];
+                } else if (nh > 1) {
+                    const float inf = __int_as_float(0x7f800000);
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) t[k] = hh[k] ? t[k] : inf;
+                    float* t0 = t;
+                    float* t1 = t + 4;
+                    int* c0 = c;
+                    int* c1 = c + 4;
+                    sort4(*reinterpret_cast<float(*)[4]>(t0), *reinterpret_cast<int(*)[4]>(c0));
+                    sort4(*reinterpret_cast<float(*)[4]>(t1), *reinterpret_cast<int(*)[4]>(c1));
+                    // odd-even merge of the two sorted halves
+                    cswap(t[0], c[0], t[4], c[4]);
+                    cswap(t[1], c[1], t[5], c[5]);
+                    cswap(t[2], c[2], t[6], c[6]);
+                    cswap(t[3], c[3], t[7], c[7]);
+                    cswap(t[2], c[2], t[4], c[4]);
+                    cswap(t[3], c[3], t[5], c[5]);
+                    cswap(t[1], c[1], t[2], c[2]);
+                    cswap(t[3], c[3], t[4], c[4]);
+                    cswap(t[5], c[5], t[6], c[6]);
+#pragma unroll
+                    for (int k = 7; k >= 1; --k)
+                        if (t[k] <= tBest) push(c[k], t[k]);
+                    ref = c[0];
+                } else if (!pop()) {
+                    return best;
+                }
+            }
+            do {
+                if (++iters > kIterBudget) { err |= DEV_ERR_BUDGET; return -1; }
+                const int code = ~ref;
+                const int first = code >> 4, cnt = code & 15;
+                switch (wr.kz) {
+                    case 0: leaf_wt<0>(S.tris, first, cnt, o, wr, tMin, tBest, best); break;
+                    case 1: leaf_wt<1>(S.tris, first, cnt, o, wr, tMin, tBest, best); break;
+                    default: leaf_wt<2>(S.tris, first, cnt, o, wr, tMin, tBest, best); break;
+                }
+                if (!pop()) return best;
+            } while (ref < 0);
+        }
+    }
+};
+
 template <>
 struct Walker<true> {
     __device__ __forceinline__ static int closest(const SceneView& S, D3 o, D3 d, double tMin, double& tBest,
