@@ -499,6 +499,9 @@ def fp64_check_leg(w, sbr, scene, n_angles: int) -> dict:
                        w["R"])
     a = sbr.run(scene, cjob, mode=sbr.MODE_BATCHED, precision=sbr.PREC_MIXED)
     b = sbr.run(scene, cjob, mode=sbr.MODE_BATCHED, precision=sbr.PREC_FP64)
+    t0 = time.perf_counter()
+    ef, ed = sbr.error_bound(scene, cjob, a)
+    bound_s = time.perf_counter() - t0
     ddb = np.abs(a.rcs_dbsm - b.rcs_dbsm)
     db64 = b.rcs_dbsm.reshape(pick.size, -1)
     lit = (db64 > db64.max(axis=0)[None, :] - 30.0).ravel()
@@ -513,6 +516,13 @@ def fp64_check_leg(w, sbr, scene, n_angles: int) -> dict:
                              "freq_ghz": float(w["freqs"][worst % len(w["freqs"])]) / 1e9,
                              "dbsm_fp64": float(b.rcs_dbsm[worst]), "dbsm_mixed": float(a.rcs_dbsm[worst])},
             "max_field_diff_rel_to_max": float(np.abs(a.field - b.field).max() / np.abs(b.field).max()),
+            "stated_error": {"what": "sbr_error_bound: per-sample bound on |dBsm - dBsm_FP64| of the mixed result",
+                             "max_db": float(ed.max()), "median_db": float(np.median(ed)),
+                             "p99_db": float(np.percentile(ed, 99)),
+                             "samples_where_bound_holds": int((ddb <= ed + 1e-9).sum()),
+                             "field_bound_holds": int((np.abs(a.field - b.field) <= ef).sum()),
+                             "median_bound_over_measured": float(np.median(ed / np.maximum(ddb, 1e-12))),
+                             "wall_s": bound_s},
             "fp64_ms": b.device_ms, "mixed_ms": a.device_ms}
 
 

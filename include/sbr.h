@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define SBR_ABI_VERSION 1
+#define SBR_ABI_VERSION 2  /* 2: sbr_config.error_bound, sbr_build_opts.node_width */
 
 /* ------------------------------------------------------------------ status */
 typedef int32_t sbr_status;
@@ -223,6 +223,26 @@ sbr_status sbr_plan_destroy(sbr_plan* plan);
 sbr_status sbr_run(sbr_scene* scene, const sbr_job* jobs, size_t n_jobs, sbr_result* out,
                    const sbr_run_opts* opts);
 
+/* ----------------------------------------------------- stated error vs FP64 */
+/* No counterpart in the reference (it has no mixed-precision mode).
+ *
+ * A bound, per sample, on how far a SBR_PREC_MIXED result of `jobs` lies from the
+ * SBR_PREC_FP64 result of the same jobs, computed by a second pass over the same
+ * rays that carries FP32 error bounds along each ray (origin and direction
+ * rounding, per-bounce drift of the hit point, path length and normal errors) and
+ * flags rays whose hit decisions lie within that uncertainty of flipping (an edge
+ * within reach of the ray, |det| near its 1e-6 threshold, t near tMin or tied with
+ * another hit); a flagged ray may add any term up to its maximum size.
+ *   field     [n_samples * 2] in: the mixed-precision fields sbr_run returned.
+ *   err_field [n_samples] out (may be NULL): bound on |field - field_FP64|.
+ *   err_db    [n_samples] out (may be NULL): bound on |dBsm - dBsm_FP64| implied by
+ *             it (dBsm floored at -100 as the reference does); +inf never occurs,
+ *             a bound above |field| gives the distance to the -100 dBsm floor.
+ * The pass costs about as much as the sweep.  opts: precision must be
+ * SBR_PREC_MIXED, polarization SBR_POL_SCALAR; the mode is ignored. */
+sbr_status sbr_error_bound(sbr_scene* scene, const sbr_job* jobs, size_t n_jobs, const sbr_run_opts* opts,
+                           const double* field, double* err_field, double* err_db);
+
 /* ------------------------------------------------------------- diagnostics */
 #define SBR_MAX_REC 16
 /* Per-ray record: the reference's hit buffers (include/app/deviceBuffers.hpp:6-15)
@@ -332,6 +352,9 @@ typedef struct sbr_config {
     int32_t csv_digits;       /* key "csv_digits" or flag --full-precision (17): significant digits
                                  of the rcs_results.csv rows; 0 -> 6, the reference's default
                                  ostream formatting */
+    int32_t error_bound;      /* key "error_bound": 1 -> RT-RCS states each row's bound on
+                                 |dBsm - dBsm_FP64| (sbr_error_bound) in a fifth column
+                                 rcs_err_db (mixed precision); 0 (default) -> the reference layout */
 } sbr_config;
 
 /* loadConfig (src/app/config.cpp:39-155): reads `default_path` (or --config),
@@ -359,6 +382,11 @@ void sbr_free(void* p);
  * double).  The header lines keep the reference's formatting. */
 sbr_status sbr_write_csv(const char* path, const sbr_config* cfg, const double* theta_deg, const double* phi_deg,
                          const double* sigma_m2, const double* rcs_dbsm, int64_t n);
+/* sbr_write_csv with a fifth column rcs_err_db (header theta,phi,rcs_m2,rcs_dbsm,rcs_err_db):
+ * each row's stated bound on |dBsm - dBsm_FP64| from sbr_error_bound. */
+sbr_status sbr_write_csv_err(const char* path, const sbr_config* cfg, const double* theta_deg,
+                             const double* phi_deg, const double* sigma_m2, const double* rcs_dbsm,
+                             const double* err_db, int64_t n);
 
 #ifdef __cplusplus
 }

@@ -309,6 +309,21 @@ def trace_records(scene: Scene, job: JobSpec, precision=PREC_MIXED, first_hit=No
     return out
 
 
+def error_bound(scene: Scene, jobs: Sequence[JobSpec] | JobSpec, result: SweepResult, stream=None):
+    """Stated error of a mixed-precision result against FP64 (sbr_error_bound):
+    (bound on |field - field_FP64| [n_samples], bound on |dBsm - dBsm_FP64|
+    [n_samples])."""
+    if isinstance(jobs, JobSpec):
+        jobs = [jobs]
+    jc = _jobs_c(jobs)
+    f = np.ascontiguousarray(np.stack([result.field.real, result.field.imag], axis=1).ravel())
+    n = f.size // 2
+    ef, ed = np.zeros(n), np.zeros(n)
+    o = _opts(MODE_BATCHED, PREC_MIXED, stream=stream)
+    check(lib().sbr_error_bound(scene.handle, jc, len(jobs), C.byref(o), _p(f), _p(ef), _p(ed)), "sbr_error_bound")
+    return ef, ed
+
+
 def trace_ray_list(scene: Scene, job: JobSpec, rays, precision=PREC_MIXED) -> np.ndarray:
     """Hit records [n] of the listed rays only, rays[k] = (angle index, i, j)
     (sbr_trace_ray_list)."""
@@ -381,11 +396,18 @@ def _load(fn: str, path: str):
     return v.reshape(-1, 3), t.reshape(-1, 3)
 
 
-def write_csv(path: str, cfg: dict, theta, phi, sigma, dbsm):
+def write_csv(path: str, cfg: dict, theta, phi, sigma, dbsm, err_db=None):
+    """rcs_results.csv in the reference layout; with err_db a fifth column rcs_err_db."""
     c = _cfg_struct(cfg)
     th, ph = np.ascontiguousarray(theta, np.float64), np.ascontiguousarray(phi, np.float64)
     s, d = np.ascontiguousarray(sigma, np.float64), np.ascontiguousarray(dbsm, np.float64)
-    check(lib().sbr_write_csv(path.encode(), C.byref(c), _p(th), _p(ph), _p(s), _p(d), th.size), "sbr_write_csv")
+    if err_db is None:
+        check(lib().sbr_write_csv(path.encode(), C.byref(c), _p(th), _p(ph), _p(s), _p(d), th.size),
+              "sbr_write_csv")
+    else:
+        e = np.ascontiguousarray(err_db, np.float64)
+        check(lib().sbr_write_csv_err(path.encode(), C.byref(c), _p(th), _p(ph), _p(s), _p(d), _p(e), th.size),
+              "sbr_write_csv_err")
 
 
 def run_sweep(cfg: dict, scene: Scene, out_csv: str | None = "rcs_results.csv", mode=None, precision=None):
@@ -394,10 +416,11 @@ def run_sweep(cfg: dict, scene: Scene, out_csv: str | None = "rcs_results.csv", 
     th, ph = config_angles(cfg)
     job = JobSpec(th, ph, [cfg["freq"]], cfg["nx"], cfg["ny"], cfg["grid_size"], cfg["max_bounces"],
                   cfg["reflection_const"])
-    res = run(scene, job, mode=cfg.get("mode", MODE_BATCHED) if mode is None else mode,
-              precision=cfg.get("precision", PREC_MIXED) if precision is None else precision)
+    prec = cfg.get("precision", PREC_MIXED) if precision is None else precision
+    res = run(scene, job, mode=cfg.get("mode", MODE_BATCHED) if mode is None else mode, precision=prec)
+    err = error_bound(scene, job, res)[1] if cfg.get("error_bound") and prec == PREC_MIXED else None
     if out_csv:
-        write_csv(out_csv, cfg, th, ph, res.sigma_m2, res.rcs_dbsm)
+        write_csv(out_csv, cfg, th, ph, res.sigma_m2, res.rcs_dbsm, err)
     return th, ph, res
 
 

@@ -131,6 +131,7 @@ class Config(C.Structure):
         ("precision", C.c_int32),
         ("mode", C.c_int32),
         ("csv_digits", C.c_int32),
+        ("error_bound", C.c_int32),
     ]
 
 
@@ -163,6 +164,7 @@ SIGNATURES = {
     "sbr_run": (_I32, [_P, _P, _SZ, _P, _P]),
     "sbr_trace_records": (_I32, [_P, _P, _P, _P]),
     "sbr_trace_ray_list": (_I32, [_P, _P, _P, _P, _SZ, _P]),
+    "sbr_error_bound": (_I32, [_P, _P, _SZ, _P, _P, _P, _P]),
     "sbr_run_noalloc": (_I32, [_P, _P, _P, _P, _P]),
     "sbr_adjoint": (_I32, [_P, _P, C.c_size_t, _P, _P, _P, _P]),
     "sbr_scene_update_vertices": (_I32, [_P, _P, _SZ]),
@@ -174,6 +176,7 @@ SIGNATURES = {
     "sbr_load_obj": (_I32, [C.c_char_p, _P, _P, _P, _P]),
     "sbr_free": (None, [_P]),
     "sbr_write_csv": (_I32, [C.c_char_p, _P, _P, _P, _P, _P, _I64]),
+    "sbr_write_csv_err": (_I32, [C.c_char_p, _P, _P, _P, _P, _P, _P, _I64]),
 }
 
 _lib = None

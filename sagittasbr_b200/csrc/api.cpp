@@ -140,6 +140,7 @@ sbr_status sbr_config_load(const char* default_path, int argc, const char* const
     if (has("precision")) c.precision = (int32_t)kv["precision"];
     if (has("engine_mode")) c.mode = (int32_t)kv["engine_mode"];
     if (has("csv_digits")) c.csv_digits = (int32_t)kv["csv_digits"];
+    if (has("error_bound")) c.error_bound = kv["error_bound"] != 0.0;
 
     bool freqCli = false;
     for (int i = 1; i < argc; ++i) {
@@ -280,6 +281,11 @@ sbr_status sbr_load_obj(const char* path, float** xyz, size_t* nverts, uint32_t*
 // --------------------------------------------------------------------- CSV
 sbr_status sbr_write_csv(const char* path, const sbr_config* c, const double* theta, const double* phi,
                          const double* sigma, const double* dbsm, int64_t n) {
+    return sbr_write_csv_err(path, c, theta, phi, sigma, dbsm, nullptr, n);
+}
+
+sbr_status sbr_write_csv_err(const char* path, const sbr_config* c, const double* theta, const double* phi,
+                             const double* sigma, const double* dbsm, const double* err_db, int64_t n) {
     if (!path || !c || (n > 0 && (!theta || !phi || !sigma || !dbsm))) return fail(SBR_ERR_INVALID_ARG, "null argument");
     if (c->csv_digits < 0 || c->csv_digits > 17) return fail(SBR_ERR_INVALID_ARG, "csv_digits must be 0..17");
     std::ofstream f(path);
@@ -287,9 +293,14 @@ sbr_status sbr_write_csv(const char* path, const sbr_config* c, const double* th
     // default ostream formatting (6 significant digits), as the reference's
     f << "# Frequency: " << c->freq << "\n# Grid: " << c->nx << "x" << c->ny << "\n";
     f << "# GridSize: " << c->grid_size << "\n# ThetaSamples: " << c->theta_samples << "\n";
-    f << "# PhiSamples: " << c->phi_samples << "\n" << "theta,phi,rcs_m2,rcs_dbsm\n";
+    f << "# PhiSamples: " << c->phi_samples << "\n"
+      << (err_db ? "theta,phi,rcs_m2,rcs_dbsm,rcs_err_db\n" : "theta,phi,rcs_m2,rcs_dbsm\n");
     if (c->csv_digits > 0) f << std::setprecision(c->csv_digits);
-    for (int64_t i = 0; i < n; ++i) f << theta[i] << "," << phi[i] << "," << sigma[i] << "," << dbsm[i] << "\n";
+    for (int64_t i = 0; i < n; ++i) {
+        f << theta[i] << "," << phi[i] << "," << sigma[i] << "," << dbsm[i];
+        if (err_db) f << "," << err_db[i];
+        f << "\n";
+    }
     if (!f.good()) return fail(SBR_ERR_IO, std::string("write failed: ") + path);
     return SBR_OK;
 }

@@ -168,6 +168,8 @@ int main(int argc, char** argv) {
     ro.mode = cfg.mode;
     ro.precision = cfg.precision;
     sbr_result res{};
+    std::vector<double> field(2 * n), err_db;
+    res.field = field.data();
     res.sigma_m2 = sigma.data();
     res.rcs_dbsm = dbsm.data();
     res.stats = stats.data();
@@ -176,7 +178,21 @@ int main(int argc, char** argv) {
         sbr_scene_destroy(scene);
         return die("sweep", st);
     }
-    st = sbr_write_csv("rcs_results.csv", &cfg, th.data(), ph.data(), sigma.data(), dbsm.data(), n);
+    // optional key error_bound: each row's stated bound against the FP64 result
+    if (cfg.error_bound) {
+        if (cfg.precision != SBR_PREC_MIXED) {
+            std::cerr << "Warning: error_bound applies to mixed precision (precision 0); not stated.\n";
+        } else {
+            err_db.resize(n);
+            st = sbr_error_bound(scene, &job, 1, &ro, field.data(), nullptr, err_db.data());
+            if (st != SBR_OK) {
+                sbr_scene_destroy(scene);
+                return die("error bound", st);
+            }
+        }
+    }
+    st = sbr_write_csv_err("rcs_results.csv", &cfg, th.data(), ph.data(), sigma.data(), dbsm.data(),
+                           err_db.empty() ? nullptr : err_db.data(), n);
     if (st != SBR_OK) {
         sbr_scene_destroy(scene);
         return die("csv", st);

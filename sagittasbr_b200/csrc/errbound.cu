@@ -1,0 +1,394 @@
+// errbound.cu -- sbr_error_bound: an a-posteriori bound, per (angle, frequency)
+// sample, on how far the mixed-precision sweep (FP32 traversal, FP64 path and
+// sums) can lie from the FP64 sweep of the same job.  No counterpart in the
+// reference, which has no mixed-precision mode.
+//
+// A second pass re-traces every ray of the plan with the mixed sweep's own
+// arithmetic (start_f and the step of ray.cuh, the watertight test of trace.cuh:
+// the same hits bit for bit) while carrying bounds on how far the FP32 ray can be
+// from the FP64 ray with the same hits:
+//   e   position error across the ray (m): origin rounding, then per bounce the
+//       lateral drift t * a, the induced change of t and the FP32 roundings;
+//   a   direction error (rad): rounding of -dir, then per reflection twice the
+//       error of the FP32 normal (8 u / sin of the triangle's corner angle) + 4 u;
+//   dL  path-length error (m): per bounce (e + t a) / |cos i| + 4 u t.
+// A ray is ambiguous when one of its decisions lies within that uncertainty of
+// flipping: a tested triangle whose edge lies within 2 (e + a D) of the ray (hit
+// or miss; D = scene diagonal, 2 covers the oblique projection of the sheared
+// test), |det| within a factor 2 of the 1e-6 threshold, or t within
+// dt = 4 m + 4 u (|o| + D) of tMin or of the current closest hit.  Boxes are widened
+// by the same margin during this pass, so a near miss inside a culled box is still
+// tested (boxes only prune; the closest hit does not change).
+// Per segment the pass sums, over rays that add a term,
+//   S1 = sum amp dL, S0 = sum (amp eps_phase + damp), damp = 2 R^n (dn_last + a),
+// and over ambiguous rays S2 = sum (amp + 2 Rmax^maxB) (the FP64 ray may add any
+// term of at most that size).  The bound on the field of frequency k is then
+//   E_k = k A / (4 pi) (2 k S1 + S0 + S2) + n_items quantum_k,
+// the last term covering the fixed-point fold of the sweep.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "plan.hpp"
+#include "ray.cuh"
+
+namespace sbr {
+namespace {
+
+constexpr float kU = 5.9604644775390625e-08f;  // 2^-24, unit roundoff of FP32
+// Phase / amplitude error of one mixed term: the FP32 remainder of 2 k L in turns
+// (2 pi 2^-25 rad), __sincosf (below 4e-7 absolute), FP32 amplitude (2^-24).
+constexpr double kPhaseEps = 1.0e-6;
+
+struct ErrParams {
+    SceneView S;
+    const Segment* segs;
+    const int64_t* seg_item_base;
+    int32_t n_segs;
+    const JobConst* jobs;
+    int64_t n_items;
+    unsigned long long* queue;
+    double* acc;       // [n_segs][4]: S1, S0, S2, ambiguous rays
+    float diag;        // scene bounding-box diagonal (m)
+    uint32_t* err;
+    const volatile int32_t* cancel;
+};
+
+__device__ __forceinline__ float norm1(F3 v) { return fabsf(v.x) + fabsf(v.y) + fabsf(v.z); }
+
+// The watertight test of trace.cuh (wt_tri, identical decisions), flagging in `amb`
+// a decision within the margin m (edges) / dt (t) of flipping.
+template <int KZ>
+__device__ __forceinline__ bool wt_tri_flag(const GTri& T, F3 o, const WtRay& w, float tMin, float tMax, float m,
+                                            float dt, float& t, bool& amb) {
+    constexpr int KX = (KZ + 1) % 3, KY = (KZ + 2) % 3;
+    const float ox = axis<KX>(o), oy = axis<KY>(o), oz = axis<KZ>(o);
+    const float az = __fsub_rn(axis<KZ>(T.v0), oz), bz = __fsub_rn(axis<KZ>(T.v1), oz),
+                cz = __fsub_rn(axis<KZ>(T.v2), oz);
+    const float ax = __fmaf_rn(-w.sx, az, __fsub_rn(axis<KX>(T.v0), ox));
+    const float ay = __fmaf_rn(-w.sy, az, __fsub_rn(axis<KY>(T.v0), oy));
+    const float bx = __fmaf_rn(-w.sx, bz, __fsub_rn(axis<KX>(T.v1), ox));
+    const float by = __fmaf_rn(-w.sy, bz, __fsub_rn(axis<KY>(T.v1), oy));
+    const float cx = __fmaf_rn(-w.sx, cz, __fsub_rn(axis<KX>(T.v2), ox));
+    const float cy = __fmaf_rn(-w.sy, cz, __fsub_rn(axis<KY>(T.v2), oy));
+    float U = __fsub_rn(__fmul_rn(cx, by), __fmul_rn(cy, bx));
+    float V = __fsub_rn(__fmul_rn(ax, cy), __fmul_rn(ay, cx));
+    float W = __fsub_rn(__fmul_rn(bx, ay), __fmul_rn(by, ax));
+    if (U == 0.0f || V == 0.0f || W == 0.0f) {
+        U = float(__dsub_rn(__dmul_rn(cx, by), __dmul_rn(cy, bx)));
+        V = float(__dsub_rn(__dmul_rn(ax, cy), __dmul_rn(ay, cx)));
+        W = float(__dsub_rn(__dmul_rn(bx, ay), __dmul_rn(by, ax)));
+    }
+    const bool inside = !((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f));
+    const float det = __fadd_rn(__fadd_rn(U, V), W);
+    // margins: distance (sheared plane) from the ray to each edge line, and t of the plane
+    const float dU = fabsf(U) * rhypotf(cx - bx, cy - by), dV = fabsf(V) * rhypotf(ax - cx, ay - cy),
+                dW = fabsf(W) * rhypotf(bx - ax, by - ay);
+    const float T3 = __fmaf_rn(U, az, __fmaf_rn(V, bz, __fmul_rn(W, cz)));
+    const float tp = det != 0.0f ? T3 * w.sz / det : 0.0f;
+    const bool inRange = tp >= tMin - dt && tp <= tMax + dt;
+    if (inRange) {
+        if (inside) {
+            if (fminf(dU, fminf(dV, dW)) < m) amb = true;
+        } else {
+            // the ray is outside across the edges whose function disagrees with the
+            // orientation; it would be inside if each of those moved by less than m
+            const bool pos = det >= 0.0f;
+            const bool vU = pos ? U < 0.0f : U > 0.0f, vV = pos ? V < 0.0f : V > 0.0f, vW = pos ? W < 0.0f : W > 0.0f;
+            if ((!vU || dU < m) && (!vV || dV < m) && (!vW || dW < m)) amb = true;
+        }
+        const float adet = fabsf(det) * w.adz;
+        if (adet >= 0.5e-6f && adet < 2.0e-6f) amb = true;
+    }
+    if (!inside) return false;
+    if (!(fabsf(det) * w.adz >= 1.0e-6f)) return false;
+    float rdet;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rdet) : "f"(det));
+    const float tt = __fmul_rn(__fmul_rn(T3, w.sz), rdet);
+    if (fabsf(tt - tMin) < dt || fabsf(tt - tMax) < dt) amb = true;
+    if (!(tt >= tMin && tt <= tMax)) return false;
+    t = tt;
+    return true;
+}
+
+template <int KZ>
+__device__ __forceinline__ void leaf_flag(const GTri* __restrict__ tris, int first, int cnt, F3 o, const WtRay& w,
+                                          float tMin, float m, float dt, float& tBest, int& best, bool& amb) {
+    for (int k = 0; k < cnt; ++k) {
+        float tt;
+        if (wt_tri_flag<KZ>(tris[first + k], o, w, tMin, tBest, m, dt, tt, amb)) {
+            tBest = tt;
+            best = first + k;
+        }
+    }
+}
+
+// Closest hit as Walker<false> finds it (4-wide nodes, watertight test), with every
+// box widened by m across the ray and dt along it, and decisions near flipping
+// flagged in `amb`.
+__device__ int closest_flag(const SceneView& S, F3 o, F3 d, float tMin, float& tBest, float m, float dt, bool& amb,
+                            uint32_t& err) {
+    const F3 inv{slab_inv(d.x), slab_inv(d.y), slab_inv(d.z)};
+    const WtRay wr = wt_ray(d);
+    const F3 oi{o.x * inv.x, o.y * inv.y, o.z * inv.z};
+    const float px = m * fabsf(inv.x), py = m * fabsf(inv.y), pz = m * fabsf(inv.z);
+    const unsigned onx = inv.x < 0.0f ? 16u : 0u, ony = inv.y < 0.0f ? 48u : 32u, onz = inv.z < 0.0f ? 80u : 64u;
+    const unsigned ofx = onx ^ 16u, ofy = ony ^ 16u, ofz = onz ^ 16u;
+    unsigned long long stack[kStackDepth];
+    int sp = 0, ref = 0, best = -1;
+    uint32_t iters = 0;
+    auto plane = [](const GNode4* p, unsigned off) {
+        return __ldg(reinterpret_cast<const float4*>(reinterpret_cast<const char*>(p) + off));
+    };
+    auto slab = [&](float nx, float fx, float ny, float fy, float nz, float fz, bool& hit) {
+        const float tn = max3f(fmaf(nx, inv.x, -oi.x) - px, fmaf(ny, inv.y, -oi.y) - py,
+                               fmaxf(fmaf(nz, inv.z, -oi.z) - pz, tMin - dt));
+        const float tf = min3f(fmaf(fx, inv.x, -oi.x) + px, fmaf(fy, inv.y, -oi.y) + py,
+                               fminf(fmaf(fz, inv.z, -oi.z) + pz, tBest + dt));
+        hit = tn <= tf * kSlabSlack;
+        return tn;
+    };
+    for (;;) {
+        while (ref >= 0) {
+            if (++iters > kIterBudget) { err |= DEV_ERR_BUDGET; return -1; }
+            const GNode4* np = S.nodes + ref;
+            const float4 nx = plane(np, onx), fx = plane(np, ofx), ny = plane(np, ony), fy = plane(np, ofy);
+            const float4 nz = plane(np, onz), fz = plane(np, ofz);
+            const int4 ch = __ldg(&np->child);
+            bool h[4];
+            float t[4] = {slab(nx.x, fx.x, ny.x, fy.x, nz.x, fz.x, h[0]), slab(nx.y, fx.y, ny.y, fy.y, nz.y, fz.y, h[1]),
+                          slab(nx.z, fx.z, ny.z, fy.z, nz.z, fz.z, h[2]), slab(nx.w, fx.w, ny.w, fy.w, nz.w, fz.w, h[3])};
+            int c[4] = {ch.x, ch.y, ch.z, ch.w};
+            const float inf = __int_as_float(0x7f800000);
+            for (int k = 0; k < 4; ++k) t[k] = h[k] ? t[k] : inf;
+            sort4(t, c);
+            for (int k = 3; k >= 0; --k)
+                if (t[k] != inf) {
+                    if (sp < kStackDepth) stack[sp++] = pack_entry(c[k], t[k]);
+                    else err |= DEV_ERR_STACK;
+                }
+            ref = -1;
+            while (sp > 0) {
+                const unsigned long long e = stack[--sp];
+                if (__uint_as_float((unsigned)(e >> 32)) <= tBest + dt) { ref = (int)(unsigned)e; break; }
+            }
+            if (ref == -1) return best;
+            while (ref < 0) {
+                if (++iters > kIterBudget) { err |= DEV_ERR_BUDGET; return -1; }
+                const int code = ~ref;
+                const int first = code >> 4, cnt = code & 15;
+                switch (wr.kz) {
+                    case 0: leaf_flag<0>(S.tris, first, cnt, o, wr, tMin, m, dt, tBest, best, amb); break;
+                    case 1: leaf_flag<1>(S.tris, first, cnt, o, wr, tMin, m, dt, tBest, best, amb); break;
+                    default: leaf_flag<2>(S.tris, first, cnt, o, wr, tMin, m, dt, tBest, best, amb); break;
+                }
+                ref = -1;
+                while (sp > 0) {
+                    const unsigned long long e = stack[--sp];
+                    if (__uint_as_float((unsigned)(e >> 32)) <= tBest + dt) { ref = (int)(unsigned)e; break; }
+                }
+                if (ref == -1) return best;
+            }
+        }
+    }
+}
+
+// One ray: the mixed sweep's path (start_f, then step_f's arithmetic per bounce)
+// with the uncertainty bounds carried along; adds the ray to the lane's sums.
+__device__ __forceinline__ void ray_bound(const ErrParams& P, const Segment& G, const JobConst& J, int i, int j,
+                                         double rmaxB, double& s1, double& s0, double& s2, unsigned& namb,
+                                         uint32_t& err) {
+    RayF r;
+    start_f<SBR_PREC_MIXED>(r, G, J, i, j);
+    float ue = 2.0f * kU * norm1(r.o);  // origin formed in FP64, rounded to FP32
+    float ua = 2.0f * kU;                // FP32 direction
+    double dL = double(kU * norm1(r.o));
+    float dnl = 0.0f;
+    bool amb = false;
+    for (int b = 0; b < J.max_bounces; ++b) {
+        const float m = 2.0f * (ue + ua * P.diag);
+        const float dt = 4.0f * m + 4.0f * kU * (norm1(r.o) + P.diag);
+        float tB = 1e20f;
+        const int slot = closest_flag(P.S, r.o, r.d, 1.0e-3f, tB, m, dt, amb, err);
+        if (slot < 0) break;
+        const GTri T = P.S.tris[slot];
+        const F3 n = f3(T.v0.w, T.v1.w, T.v2.w);
+        // the step of step_f (ray.cuh), operation for operation
+        r.cosl = dot(n, f3(-r.d.x, -r.d.y, -r.d.z));
+        r.nl = n;
+        r.dl = r.d;
+        ++r.count;
+        r.L += double(tB);
+        const F3 p = r.o + tB * r.d;
+        const float dn = 2.0f * dot(r.d, n);
+        r.d = unit(r.d - dn * n);
+        r.o = p + 1.0e-4f * n;
+        // uncertainty of this bounce
+        const F3 e1 = f3(T.v1.x - T.v0.x, T.v1.y - T.v0.y, T.v1.z - T.v0.z);
+        const F3 e2 = f3(T.v2.x - T.v0.x, T.v2.y - T.v0.y, T.v2.z - T.v0.z);
+        const F3 N = cross(e1, e2);
+        const float sinang = sqrtf(dot(N, N) / fmaxf(dot(e1, e1) * dot(e2, e2), 1e-30f));
+        const float dnrm = 8.0f * kU / fmaxf(sinang, 1e-6f);
+        const float ci = fmaxf(fabsf(r.cosl), 1e-6f);
+        const float dtb = (ue + tB * ua) / ci + 4.0f * kU * tB;
+        dL += double(dtb);
+        ue = ue + tB * ua + dtb + 2.0f * kU * norm1(p) + 1.0e-4f * dnrm;
+        ua = ua + 2.0f * dnrm + 4.0f * kU;
+        dnl = dnrm;
+    }
+    float Rn = 1.0f;
+    for (int b = 0; b < r.count; ++b) Rn *= J.reflf;
+    const float amp = (r.count > 0 && r.cosl > 0.0f) ? 2.0f * r.cosl * Rn : 0.0f;
+    if (amb) {
+        s2 += double(amp) + 2.0 * rmaxB;
+        ++namb;
+    } else if (r.count > 0) {
+        s1 += double(amp) * dL;
+        s0 += double(amp) * kPhaseEps + 2.0 * double(fabsf(Rn)) * double(dnl + ua);
+    }
+}
+
+__global__ void __launch_bounds__(kCtaThreads) k_errbound(const ErrParams P) {
+    constexpr unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    uint32_t err = 0;
+    for (;;) {
+        long long item = 0;
+        if (lane == 0) {
+            item = (long long)atomicAdd(P.queue, 1ull);
+            if (item < P.n_items && P.cancel && *P.cancel != 0) {
+                atomicOr(P.err, DEV_ERR_CANCEL);
+                item = P.n_items;
+            }
+        }
+        item = __shfl_sync(FULL, item, 0);
+        if (item >= P.n_items) break;
+        const int seg = find_segment(P.seg_item_base, P.n_segs, item);
+        const Segment& G = P.segs[seg];
+        const JobConst J = P.jobs[G.job];
+        const double rmaxB = pow(fmax(1.0, fabs(J.refl)), double(J.max_bounces));
+        const int b0 = int(item - G.item_base) * G.blocks_per_item;
+        const int b1 = min(b0 + G.blocks_per_item, G.blocks);
+        double s1 = 0.0, s0 = 0.0, s2 = 0.0;
+        unsigned namb = 0;
+        for (int blk = b0; blk < b1; ++blk) {
+            const int i = G.i0 + (blk % G.blocks_x) * kBlockW + (lane % kBlockW);
+            const int j = G.j0 + (blk / G.blocks_x) * kBlockH + (lane / kBlockW);
+            if (i < G.i0 + G.ni && j < G.j0 + G.nj) ray_bound(P, G, J, i, j, rmaxB, s1, s0, s2, namb, err);
+        }
+        for (int off = 16; off > 0; off >>= 1) {
+            s1 += __shfl_xor_sync(FULL, s1, off);
+            s0 += __shfl_xor_sync(FULL, s0, off);
+            s2 += __shfl_xor_sync(FULL, s2, off);
+        }
+        namb = __reduce_add_sync(FULL, namb);
+        if (lane == 0) {
+            atomicAdd(P.acc + 4 * seg, s1);
+            atomicAdd(P.acc + 4 * seg + 1, s0);
+            atomicAdd(P.acc + 4 * seg + 2, s2);
+            atomicAdd(P.acc + 4 * seg + 3, double(namb));
+        }
+    }
+    if (err) atomicOr(P.err, err);
+}
+
+}  // namespace
+}  // namespace sbr
+
+extern "C" sbr_status sbr_error_bound(sbr_scene* s, const sbr_job* jobs, size_t n_jobs, const sbr_run_opts* opts,
+                                      const double* field, double* err_field, double* err_db) {
+    using namespace sbr;
+    if (!s || (!jobs && n_jobs) || !field) return fail(SBR_ERR_INVALID_ARG, "scene, jobs and field are required");
+    sbr_run_opts o{};
+    if (opts) o = *opts;
+    if (o.precision != SBR_PREC_MIXED)
+        return fail(SBR_ERR_UNSUPPORTED, "the error bound is stated for SBR_PREC_MIXED results");
+    if (o.polarization != SBR_POL_SCALAR) return fail(SBR_ERR_UNSUPPORTED, "the error bound covers the scalar field");
+    o.mode = SBR_MODE_BATCHED;
+    o.first_hit = SBR_FIRST_HIT_TRAVERSE;
+    o.use_graph = 0;
+    o.autotune = 0;
+    DeviceGuard device_guard;
+    SBR_CUDA(cudaSetDevice(s->device));
+    sbr_plan* p = nullptr;
+    sbr_status st = sbr_plan_create(s, jobs, n_jobs, &o, &p);
+    if (st != SBR_OK) return st;
+    double* d_acc = nullptr;
+    unsigned long long* d_queue = nullptr;
+    std::vector<double> acc(4 * (size_t)std::max<int64_t>(p->n_segs, 1), 0.0);
+    cudaError_t e = cudaMalloc(&d_acc, acc.size() * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&d_queue, sizeof(unsigned long long));
+    if (e != cudaSuccess) st = fail(SBR_ERR_OOM, "error-bound accumulators");
+    if (st == SBR_OK) {
+        e = cudaMemsetAsync(d_acc, 0, acc.size() * sizeof(double), p->stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(d_queue, 0, sizeof(unsigned long long), p->stream);
+        if (e != cudaSuccess) st = cuda_fail(e, "error-bound clear");
+    }
+    if (st == SBR_OK && p->n_items > 0) {
+        ErrParams P{};
+        P.S = s->view();
+        P.segs = p->d_segs;
+        P.seg_item_base = p->d_seg_base;
+        P.n_segs = (int32_t)p->n_segs;
+        P.jobs = p->d_jobs;
+        P.n_items = p->n_items;
+        P.queue = d_queue;
+        P.acc = d_acc;
+        const double dx = s->aabb_hi[0] - s->aabb_lo[0], dy = s->aabb_hi[1] - s->aabb_lo[1],
+                     dz = s->aabb_hi[2] - s->aabb_lo[2];
+        P.diag = float(std::sqrt(dx * dx + dy * dy + dz * dz));
+        P.err = p->d_err;
+        P.cancel = p->d_cancel;
+        int occ = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_errbound, kCtaThreads, 0);
+        if (e != cudaSuccess) st = cuda_fail(e, "occupancy");
+        if (st == SBR_OK) {
+            const long long grid = std::min<long long>((long long)std::max(occ, 1) * p->num_sms, (p->n_items + 3) / 4);
+            k_errbound<<<(unsigned)std::max(grid, 1LL), kCtaThreads, 0, p->stream>>>(P);
+            e = cudaGetLastError();
+            if (e == cudaSuccess) e = cudaStreamSynchronize(p->stream);
+            if (e != cudaSuccess) st = cuda_fail(e, "error-bound pass");
+        }
+        if (st == SBR_OK) {
+            uint32_t de = 0;
+            e = cudaMemcpy(&de, p->d_err, sizeof(de), cudaMemcpyDeviceToHost);
+            if (e != cudaSuccess) st = cuda_fail(e, "error word");
+            else if (de) {
+                cudaMemset(p->d_err, 0, sizeof(de));
+                st = (de & DEV_ERR_CANCEL) ? fail(SBR_ERR_CANCELLED, "run cancelled")
+                     : (de & DEV_ERR_BUDGET) ? fail(SBR_ERR_TIMEOUT, "traversal iteration budget exceeded")
+                                             : fail(SBR_ERR_STACK, "traversal stack overflow");
+            }
+        }
+    }
+    if (st == SBR_OK) {
+        e = cudaMemcpy(acc.data(), d_acc, acc.size() * sizeof(double), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) st = cuda_fail(e, "error-bound copy");
+    }
+    if (st == SBR_OK) {
+        for (int64_t g = 0; g < p->n_segs; ++g) {
+            const Segment& G = p->segs[(size_t)g];
+            const JobConst& J = p->jobs[(size_t)G.job];
+            const int64_t items = p->seg_base[(size_t)g + 1] - p->seg_base[(size_t)g];
+            for (int k = 0; k < J.n_freqs; ++k) {
+                const FreqConst& F = p->freqs[(size_t)(J.freq_base + k)];
+                const int64_t smp = G.sample_base + k;
+                const double E = F.scale * (2.0 * F.k * acc[4 * g] + acc[4 * g + 1] + acc[4 * g + 2]) +
+                                 double(items + 1) * F.quantum;
+                const double a = std::hypot(field[2 * smp], field[2 * smp + 1]);
+                if (err_field) err_field[smp] = E;
+                if (err_db) {
+                    const double db = 10.0 * std::log10(std::max(4.0 * M_PI * a * a, 1e-10));
+                    const double hi = 10.0 * std::log10(std::max(4.0 * M_PI * (a + E) * (a + E), 1e-10));
+                    const double lo_a = std::max(a - E, 0.0);
+                    const double lo = 10.0 * std::log10(std::max(4.0 * M_PI * lo_a * lo_a, 1e-10));
+                    err_db[smp] = std::max(hi - db, db - lo);
+                }
+            }
+        }
+    }
+    cudaFree(d_acc);
+    cudaFree(d_queue);
+    sbr_plan_destroy(p);
+    return st;
+}

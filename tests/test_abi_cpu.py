@@ -68,7 +68,7 @@ def test_status_strings():
     for code, name in _lib.STATUS_NAMES.items():
         assert L.sbr_status_str(code).decode() == name
     assert L.sbr_status_str(999) == b"SBR_ERR_UNKNOWN"
-    assert L.sbr_abi_version() == 1
+    assert L.sbr_abi_version() == 2
 
 
 REF_STYLE_CONFIG = """# angular sampling
@@ -210,3 +210,20 @@ def test_reference_gpu_build_loads():
         if not ref_gpu.available(bits):
             pytest.skip("reference GPU build not present")
         assert ref_gpu.lib(bits).sbrref_gpu_real_bits() == bits
+
+
+def test_csv_error_column(tmp_path):
+    """error_bound 1 (config key): rcs_results.csv gains a fifth column rcs_err_db;
+    without it the layout is the reference's."""
+    (tmp_path / "config.txt").write_text("error_bound 1\nphi_samples 2\n")
+    cfg = sbr.load_config(str(tmp_path / "config.txt"))
+    assert cfg["error_bound"] == 1
+    assert sbr.load_config(str(tmp_path / "none"))["error_bound"] == 0
+    th, ph = np.array([90.0, 90.0]), np.array([0.0, 180.0])
+    p = tmp_path / "rcs_results.csv"
+    sbr.write_csv(str(p), cfg, th, ph, np.array([1.0, 2.0]), np.array([0.0, 3.0103]), np.array([0.01, 0.25]))
+    lines = p.read_text().splitlines()
+    assert lines[5] == "theta,phi,rcs_m2,rcs_dbsm,rcs_err_db"
+    assert lines[6].split(",")[-1] == "0.01" and lines[7].split(",")[-1] == "0.25"
+    sbr.write_csv(str(p), cfg, th, ph, np.array([1.0, 2.0]), np.array([0.0, 3.0103]))
+    assert p.read_text().splitlines()[5] == "theta,phi,rcs_m2,rcs_dbsm"
