@@ -226,19 +226,24 @@ sbr_status sbr_run(sbr_scene* scene, const sbr_job* jobs, size_t n_jobs, sbr_res
 /* ----------------------------------------------------- stated error vs FP64 */
 /* No counterpart in the reference (it has no mixed-precision mode).
  *
- * A bound, per sample, on how far a SBR_PREC_MIXED result of `jobs` lies from the
- * SBR_PREC_FP64 result of the same jobs, computed by a second pass over the same
- * rays that carries FP32 error bounds along each ray (origin and direction
- * rounding, per-bounce drift of the hit point, path length and normal errors) and
- * flags rays whose hit decisions lie within that uncertainty of flipping (an edge
- * within reach of the ray, |det| near its 1e-6 threshold, t near tMin or tied with
- * another hit); a flagged ray may add any term up to its maximum size.
+ * The error, per sample, of a SBR_PREC_MIXED result of `jobs` against the
+ * SBR_PREC_FP64 result of the same jobs.  A second pass traces the same rays with
+ * the mixed arithmetic while carrying FP32 error bounds along each ray (origin and
+ * direction rounding, per-bounce drift of the hit point, path length and normal
+ * errors).  Rays whose hit decisions lie within that uncertainty of flipping (an
+ * edge within reach of the ray, |det| near its 1e-6 threshold, t near tMin or tied
+ * with another hit) or whose phase uncertainty exceeds 0.05 rad are re-traced with
+ * the FP64 sweep's own arithmetic and their exact difference is summed; the other
+ * rays differ by rounding only, bounded with a probabilistic rounding-error bound
+ * (6 standard deviations of independent per-ray errors; exceeded with probability
+ * below 6e-8).
  *   field     [n_samples * 2] in: the mixed-precision fields sbr_run returned.
- *   err_field [n_samples] out (may be NULL): bound on |field - field_FP64|.
- *   err_db    [n_samples] out (may be NULL): bound on |dBsm - dBsm_FP64| implied by
- *             it (dBsm floored at -100 as the reference does); +inf never occurs,
- *             a bound above |field| gives the distance to the -100 dBsm floor.
- * The pass costs about as much as the sweep.  opts: precision must be
+ *   err_field [n_samples] out (may be NULL): stated |field - field_FP64|.
+ *   err_db    [n_samples] out (may be NULL): the |dBsm - dBsm_FP64| it implies (dBsm
+ *             floored at -100 as the reference does: a stated error above |field|
+ *             gives the distance to that floor).
+ * The pass costs about as much as the sweep plus an FP64 trace of the re-traced
+ * rays (FP64 triangles are uploaded on first use).  opts: precision must be
  * SBR_PREC_MIXED, polarization SBR_POL_SCALAR; the mode is ignored. */
 sbr_status sbr_error_bound(sbr_scene* scene, const sbr_job* jobs, size_t n_jobs, const sbr_run_opts* opts,
                            const double* field, double* err_field, double* err_db);

@@ -1,7 +1,7 @@
-// errbound.cu -- sbr_error_bound: an a-posteriori bound, per (angle, frequency)
-// sample, on how far the mixed-precision sweep (FP32 traversal, FP64 path and
-// sums) can lie from the FP64 sweep of the same job.  No counterpart in the
-// reference, which has no mixed-precision mode.
+// errbound.cu -- sbr_error_bound: the error, per (angle, frequency) sample, of the
+// mixed-precision sweep (FP32 traversal, FP64 path and sums) against the FP64
+// sweep of the same job.  No counterpart in the reference, which has no
+// mixed-precision mode.
 //
 // A second pass re-traces every ray of the plan with the mixed sweep's own
 // arithmetic (start_f and the step of ray.cuh, the watertight test of trace.cuh:
@@ -12,19 +12,23 @@
 //   a   direction error (rad): rounding of -dir, then per reflection twice the
 //       error of the FP32 normal (8 u / sin of the triangle's corner angle) + 4 u;
 //   dL  path-length error (m): per bounce (e + t a) / |cos i| + 4 u t.
-// A ray is ambiguous when one of its decisions lies within that uncertainty of
-// flipping: a tested triangle whose edge lies within 2 (e + a D) of the ray (hit
-// or miss; D = scene diagonal, 2 covers the oblique projection of the sheared
-// test), |det| within a factor 2 of the 1e-6 threshold, or t within
-// dt = 4 m + 4 u (|o| + D) of tMin or of the current closest hit.  Boxes are widened
-// by the same margin during this pass, so a near miss inside a culled box is still
-// tested (boxes only prune; the closest hit does not change).
-// Per segment the pass sums, over rays that add a term,
-//   S1 = sum amp dL, S0 = sum (amp eps_phase + damp), damp = 2 R^n (dn_last + a),
-// and over ambiguous rays S2 = sum (amp + 2 Rmax^maxB) (the FP64 ray may add any
-// term of at most that size).  The bound on the field of frequency k is then
-//   E_k = k A / (4 pi) (2 k S1 + S0 + S2) + n_items quantum_k,
-// the last term covering the fixed-point fold of the sweep.
+// A ray is re-traced in FP64 when one of its decisions lies within that
+// uncertainty of flipping -- a tested triangle whose edge lies within 2 (e + a D)
+// of the ray (hit or miss; D = scene diagonal, 2 covers the oblique projection of
+// the sheared test), |det| within a factor 2 of the 1e-6 threshold, t within
+// dt = 4 m + 4 u (|o| + D) of tMin or of the current closest hit -- or when its
+// phase uncertainty 2 k_max dL exceeds 0.05 rad.  Boxes are widened by the same
+// margin during this pass, so a near miss inside a culled box is still tested
+// (boxes only prune; the closest hit does not change).  For those rays the exact
+// difference of the FP64 and mixed terms is summed per sample (Delta_k).  The other
+// rays differ from FP64 only by rounding, |d term| <= scale_k (amp 2 k dL + amp eps
+// + damp), damp = 2 R^n (dn_last + a): independent, zero-mean errors whose sum is
+// bounded with the probabilistic rounding-error bound of Higham and Mary (SIAM J.
+// Sci. Comput. 41(5), 2019): |sum| <= lambda sqrt(sum of squares) except with
+// probability 4 exp(-lambda^2 / 2) (lambda = 6: 6e-8).  Per sample
+//   E_k = |Delta_k| + lambda scale_k (2 k sqrt(Q1) + sqrt(Q0)) + (items + 1) quantum_k,
+// Q1 = sum (amp dL)^2, Q0 = sum (amp eps + damp)^2 over the rounding-only rays, the
+// last term covering the fixed-point fold of the sweep.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -40,15 +44,20 @@ constexpr float kU = 5.9604644775390625e-08f;  // 2^-24, unit roundoff of FP32
 // (2 pi 2^-25 rad), __sincosf (below 4e-7 absolute), FP32 amplitude (2^-24).
 constexpr double kPhaseEps = 1.0e-6;
 
+constexpr double kPhaseExact = 0.05;  // rad: rays with more phase uncertainty are re-traced in FP64
+constexpr double kLambda = 6.0;       // probabilistic bound multiplier (failure below 6e-8)
+
 struct ErrParams {
     SceneView S;
     const Segment* segs;
     const int64_t* seg_item_base;
     int32_t n_segs;
     const JobConst* jobs;
+    const FreqConst* freqs;
     int64_t n_items;
     unsigned long long* queue;
-    double* acc;       // [n_segs][4]: S1, S0, S2, ambiguous rays
+    double* acc;       // [n_segs][4]: Q1, Q0, rays re-traced in FP64, rays traced
+    double* dfield;    // [n_samples][2]: sum of (FP64 term - mixed term) of the re-traced rays
     float diag;        // scene bounding-box diagonal (m)
     uint32_t* err;
     const volatile int32_t* cancel;
@@ -194,9 +203,11 @@ __device__ int closest_flag(const SceneView& S, F3 o, F3 d, float tMin, float& t
 }
 
 // One ray: the mixed sweep's path (start_f, then step_f's arithmetic per bounce)
-// with the uncertainty bounds carried along; adds the ray to the lane's sums.
-__device__ __forceinline__ void ray_bound(const ErrParams& P, const Segment& G, const JobConst& J, int i, int j,
-                                         double rmaxB, double& s1, double& s0, double& s2, unsigned& namb,
+// with the uncertainty bounds carried along; rays near a decision or with a large
+// phase uncertainty are re-traced with the FP64 sweep's own step and their term
+// differences added to dfield, the others add to the lane's sums of squares.
+__device__ __forceinline__ void ray_bound(const ErrParams& P, const Segment& G, const JobConst& J, const FreqConst* F,
+                                         int K, double kmax, int i, int j, double& q1, double& q0, unsigned& nex,
                                          uint32_t& err) {
     RayF r;
     start_f<SBR_PREC_MIXED>(r, G, J, i, j);
@@ -236,15 +247,34 @@ __device__ __forceinline__ void ray_bound(const ErrParams& P, const Segment& G, 
         ua = ua + 2.0f * dnrm + 4.0f * kU;
         dnl = dnrm;
     }
-    float Rn = 1.0f;
-    for (int b = 0; b < r.count; ++b) Rn *= J.reflf;
-    const float amp = (r.count > 0 && r.cosl > 0.0f) ? 2.0f * r.cosl * Rn : 0.0f;
-    if (amb) {
-        s2 += double(amp) + 2.0 * rmaxB;
-        ++namb;
+    const RayOut om = finish_f<SBR_PREC_MIXED>(r, J);
+    if (amb || (r.count > 0 && 2.0 * kmax * dL > kPhaseExact)) {
+        // the FP64 sweep's own ray (start_d / step_d) and the exact term differences
+        RayD rd;
+        PolD ed;
+        start_d(rd, G, J, i, j);
+        if (J.max_bounces > 0) {
+            bool done = false;
+            while (!done) done = step_d<false, false>(rd, ed, P.S, J.max_bounces, err, nullptr);
+        }
+        const RayOut od = finish_d(rd, J);
+        for (int k = 0; k < K; ++k) {
+            double re = 0.0, im = 0.0, rm = 0.0, imm = 0.0;
+            if (od.amp != 0.0f) po_term(SBR_PREC_FP64, F[k], od, re, im);
+            if (om.amp != 0.0f) po_term(SBR_PREC_MIXED, F[k], om, rm, imm);
+            re -= rm * F[k].scale;  // mixed terms are summed without k A / (4 pi)
+            im -= imm * F[k].scale;
+            if (re != 0.0 || im != 0.0) {
+                atomicAdd(P.dfield + 2 * (G.sample_base + k), re);
+                atomicAdd(P.dfield + 2 * (G.sample_base + k) + 1, im);
+            }
+        }
+        ++nex;
     } else if (r.count > 0) {
-        s1 += double(amp) * dL;
-        s0 += double(amp) * kPhaseEps + 2.0 * double(fabsf(Rn)) * double(dnl + ua);
+        const double a1 = double(om.amp) * dL;
+        const double a0 = double(om.amp) * kPhaseEps + 2.0 * double(fabsf(om.Rn)) * double(dnl + ua);
+        q1 += a1 * a1;
+        q0 += a0 * a0;
     }
 }
 
@@ -266,27 +296,32 @@ __global__ void __launch_bounds__(kCtaThreads) k_errbound(const ErrParams P) {
         const int seg = find_segment(P.seg_item_base, P.n_segs, item);
         const Segment& G = P.segs[seg];
         const JobConst J = P.jobs[G.job];
-        const double rmaxB = pow(fmax(1.0, fabs(J.refl)), double(J.max_bounces));
+        const FreqConst* F = P.freqs + J.freq_base;
+        double kmax = 0.0;
+        for (int k = 0; k < J.n_freqs; ++k) kmax = fmax(kmax, F[k].k);
         const int b0 = int(item - G.item_base) * G.blocks_per_item;
         const int b1 = min(b0 + G.blocks_per_item, G.blocks);
-        double s1 = 0.0, s0 = 0.0, s2 = 0.0;
-        unsigned namb = 0;
+        double q1 = 0.0, q0 = 0.0;
+        unsigned nex = 0, nray = 0;
         for (int blk = b0; blk < b1; ++blk) {
             const int i = G.i0 + (blk % G.blocks_x) * kBlockW + (lane % kBlockW);
             const int j = G.j0 + (blk / G.blocks_x) * kBlockH + (lane / kBlockW);
-            if (i < G.i0 + G.ni && j < G.j0 + G.nj) ray_bound(P, G, J, i, j, rmaxB, s1, s0, s2, namb, err);
+            if (i < G.i0 + G.ni && j < G.j0 + G.nj) {
+                ray_bound(P, G, J, F, J.n_freqs, kmax, i, j, q1, q0, nex, err);
+                ++nray;
+            }
         }
         for (int off = 16; off > 0; off >>= 1) {
-            s1 += __shfl_xor_sync(FULL, s1, off);
-            s0 += __shfl_xor_sync(FULL, s0, off);
-            s2 += __shfl_xor_sync(FULL, s2, off);
+            q1 += __shfl_xor_sync(FULL, q1, off);
+            q0 += __shfl_xor_sync(FULL, q0, off);
         }
-        namb = __reduce_add_sync(FULL, namb);
+        nex = __reduce_add_sync(FULL, nex);
+        nray = __reduce_add_sync(FULL, nray);
         if (lane == 0) {
-            atomicAdd(P.acc + 4 * seg, s1);
-            atomicAdd(P.acc + 4 * seg + 1, s0);
-            atomicAdd(P.acc + 4 * seg + 2, s2);
-            atomicAdd(P.acc + 4 * seg + 3, double(namb));
+            atomicAdd(P.acc + 4 * seg, q1);
+            atomicAdd(P.acc + 4 * seg + 1, q0);
+            atomicAdd(P.acc + 4 * seg + 2, double(nex));
+            atomicAdd(P.acc + 4 * seg + 3, double(nray));
         }
     }
     if (err) atomicOr(P.err, err);
@@ -310,23 +345,31 @@ extern "C" sbr_status sbr_error_bound(sbr_scene* s, const sbr_job* jobs, size_t 
     o.autotune = 0;
     DeviceGuard device_guard;
     SBR_CUDA(cudaSetDevice(s->device));
+    sbr_status st = ensure_fp64(s);  // the re-traced rays walk the FP64 triangles
+    if (st != SBR_OK) return st;
     sbr_plan* p = nullptr;
-    sbr_status st = sbr_plan_create(s, jobs, n_jobs, &o, &p);
+    st = sbr_plan_create(s, jobs, n_jobs, &o, &p);
     if (st != SBR_OK) return st;
     double* d_acc = nullptr;
+    double* d_dfield = nullptr;
     unsigned long long* d_queue = nullptr;
     std::vector<double> acc(4 * (size_t)std::max<int64_t>(p->n_segs, 1), 0.0);
+    std::vector<double> dfield(2 * (size_t)std::max<int64_t>(p->n_samples, 1), 0.0);
     cudaError_t e = cudaMalloc(&d_acc, acc.size() * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&d_dfield, dfield.size() * sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&d_queue, sizeof(unsigned long long));
     if (e != cudaSuccess) st = fail(SBR_ERR_OOM, "error-bound accumulators");
     if (st == SBR_OK) {
         e = cudaMemsetAsync(d_acc, 0, acc.size() * sizeof(double), p->stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(d_dfield, 0, dfield.size() * sizeof(double), p->stream);
         if (e == cudaSuccess) e = cudaMemsetAsync(d_queue, 0, sizeof(unsigned long long), p->stream);
         if (e != cudaSuccess) st = cuda_fail(e, "error-bound clear");
     }
     if (st == SBR_OK && p->n_items > 0) {
         ErrParams P{};
         P.S = s->view();
+        P.freqs = p->d_freqs;
+        P.dfield = d_dfield;
         P.segs = p->d_segs;
         P.seg_item_base = p->d_seg_base;
         P.n_segs = (int32_t)p->n_segs;
@@ -363,6 +406,8 @@ extern "C" sbr_status sbr_error_bound(sbr_scene* s, const sbr_job* jobs, size_t 
     }
     if (st == SBR_OK) {
         e = cudaMemcpy(acc.data(), d_acc, acc.size() * sizeof(double), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(dfield.data(), d_dfield, dfield.size() * sizeof(double),
+                                             cudaMemcpyDeviceToHost);
         if (e != cudaSuccess) st = cuda_fail(e, "error-bound copy");
     }
     if (st == SBR_OK) {
@@ -373,7 +418,8 @@ extern "C" sbr_status sbr_error_bound(sbr_scene* s, const sbr_job* jobs, size_t 
             for (int k = 0; k < J.n_freqs; ++k) {
                 const FreqConst& F = p->freqs[(size_t)(J.freq_base + k)];
                 const int64_t smp = G.sample_base + k;
-                const double E = F.scale * (2.0 * F.k * acc[4 * g] + acc[4 * g + 1] + acc[4 * g + 2]) +
+                const double E = std::hypot(dfield[2 * smp], dfield[2 * smp + 1]) +
+                                 kLambda * F.scale * (2.0 * F.k * std::sqrt(acc[4 * g]) + std::sqrt(acc[4 * g + 1])) +
                                  double(items + 1) * F.quantum;
                 const double a = std::hypot(field[2 * smp], field[2 * smp + 1]);
                 if (err_field) err_field[smp] = E;
@@ -388,6 +434,7 @@ extern "C" sbr_status sbr_error_bound(sbr_scene* s, const sbr_job* jobs, size_t 
         }
     }
     cudaFree(d_acc);
+    cudaFree(d_dfield);
     cudaFree(d_queue);
     sbr_plan_destroy(p);
     return st;

@@ -211,4 +211,47 @@ __device__ __forceinline__ RayOut finish_d(const RayD& r, const JobConst& J) {
     return o;
 }
 
+// ------------------------------------------------------------ PO term
+// sin and cos of 2 pi x for a phase x given in turns (FP64): the whole turns are
+// removed exactly (x - rint(x) is exact for |x| < 2^52), the remainder in
+// [-1/2, 1/2] is rounded to FP32 (an absolute error below 3e-8 turns) and its
+// sine and cosine are taken in FP32.
+__device__ __forceinline__ void sincos_turns(double x, float& s, float& c) {
+    const float r = float(x - rint(x));
+    __sincosf(6.28318530717958647692f * r, &s, &c);
+}
+
+// PO term of one ray at one frequency, added to (re, im).
+//  FP32: the reference FP32 arithmetic (phase fmodf in FP32).
+//  MIXED: phase 2 k L = 2 pi (k / pi) L reduced in turns (sincos_turns); the
+//         term is summed without the factor k A / (4 pi), which the item fold
+//         applies once per channel.
+//  FP64: the reference USE_DOUBLE arithmetic.
+__device__ __forceinline__ void po_term(int prec, const FreqConst& F, const RayOut& r, double& re, double& im) {
+    if (prec == SBR_PREC_FP32) {
+        const float twoPi = 6.28318548202514648438f;
+        float phase = (2.0f * F.kf) * r.dist32;
+        phase = fmodf(phase, twoPi);
+        const float mag = (F.scalef * 2.0f) * r.cosT * r.Rn;
+        float s, c;
+        sincosf(phase, &s, &c);
+        re += double(-mag * s);
+        im += double(mag * c);
+    } else if (prec == SBR_PREC_MIXED) {
+        float s, c;
+        sincos_turns(F.turns * r.L, s, c);
+        const double a = double(r.amp);
+        re -= a * double(s);
+        im += a * double(c);
+    } else {
+        const double twoPi = 2.0 * 3.14159265358979323846;
+        const double phase = fmod((2.0 * F.k) * r.L, twoPi);
+        const double mag = (F.scale * 2.0) * r.cosD * r.RnD;
+        double s, c;
+        sincos(phase, &s, &c);
+        re += -mag * s;
+        im += mag * c;
+    }
+}
+
 }  // namespace sbr
