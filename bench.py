@@ -151,11 +151,21 @@ def ref_gpu_leg(w, sbr, scene, value):
         db64 = 10 * np.log10(np.maximum(ours64.sigma_m2.reshape(ref_s.shape), 1e-10))
         lit = db_ref > db_ref.max(axis=0)[None, :] - 30.0
         d, d64 = np.abs(db - db_ref), np.abs(db64 - db_ref)
+        # the engine's stated error of its mixed result against FP64 on the same samples
+        _, ed = sbr.error_bound(scene, job, ours)
+        ed = ed.reshape(ref_s.shape)
+        over = d > 0.1
         out["fp64_build_vs_engine"] = {
             "samples": int(ref_s.size), "theta": list(th64), "phi": list(ph64), "grid": w["nx"],
             "mixed_max_abs_ddb": float(d.max()), "mixed_frac_within_0.1dB": float((d <= 0.1).mean()),
             "mixed_max_abs_ddb_within_30dB_of_peak": float(d[lit].max()),
             "fp64_max_abs_ddb": float(d64.max()),
+            "mixed_samples_over_0.1dB": int(over.sum()),
+            "mixed_over_0.1dB_within_stated_error_plus_fp64_gap": int((d[over] <= ed[over] + d64[over] + 1e-9).sum()),
+            "mixed_over_0.1dB_detail": [{"ddb": float(d[q]), "stated_db": float(ed[q]), "fp64_gap_db": float(d64[q]),
+                                         "dbsm_ref": float(db_ref[q]), "db_below_peak": float(
+                                             db_ref.max(axis=0)[q[1]] - db_ref[q])}
+                                        for q in zip(*np.nonzero(over))][:8],
             "fp64_max_rel_sigma_diff_within_30dB_of_peak": float(
                 (np.abs(ours64.sigma_m2.reshape(ref_s.shape) - ref_s) / ref_s)[lit].max()),
             "ref_fp64_wall_s": float(r64["wall_s"].sum())}
