@@ -3,7 +3,9 @@
 frequency, 5 bounces.
 
 * mixed precision against the engine's FP64 mode: within 0.1 dB on every sample
-  within 30 dB of its frequency's strongest sample (the engine's accuracy bar);
+  within 30 dB of its frequency's strongest sample (the engine's accuracy bar), and
+  on every sample, unfiltered, within the error the engine states for it
+  (sbr_error_bound);
 * mixed precision against the reference's own USE_DOUBLE GPU build (baseline/_ref)
   on two azimuths, same bar;
 * the batched trace equals per-frequency traces on the same grid (one trace serves
@@ -31,9 +33,10 @@ def aircraft():
         job = sbr.JobSpec([90.0] * len(AZ), AZ, FREQS, n, n, G, 5)
         mixed = sbr.run(sc, job, precision=sbr.PREC_MIXED)
         fp64 = sbr.run(sc, job, precision=sbr.PREC_FP64)
+        err_field, err_db = sbr.error_bound(sc, job, mixed)
         per_f = [sbr.run(sc, sbr.JobSpec([90.0] * len(AZ), AZ, [f], n, n, G, 5), precision=sbr.PREC_MIXED)
                  for f in FREQS[::3]]
-    return dict(v=v, t=t, G=G, n=n, mixed=mixed, fp64=fp64, per_f=per_f)
+    return dict(v=v, t=t, G=G, n=n, mixed=mixed, fp64=fp64, per_f=per_f, err_field=err_field, err_db=err_db)
 
 
 def _db(s):
@@ -47,6 +50,15 @@ def test_mixed_within_0p1_db_of_fp64(aircraft):
     err = np.abs(m - d)[lit]
     print(f"aircraft mixed vs FP64: max |d dB| {err.max():.2e} over {lit.sum()} samples")
     assert err.max() <= 0.1
+
+
+def test_mixed_unfiltered_within_stated_error(aircraft):
+    df = np.abs(aircraft["mixed"].field - aircraft["fp64"].field)
+    ddb = np.abs(aircraft["mixed"].rcs_dbsm - aircraft["fp64"].rcs_dbsm)
+    print(f"aircraft unfiltered: max |d dB| {ddb.max():.2e}, stated max {aircraft['err_db'].max():.2e}, "
+          f"median {np.median(aircraft['err_db']):.2e}")
+    assert np.all(df <= aircraft["err_field"])
+    assert np.all(ddb <= aircraft["err_db"] + 1e-9)
 
 
 def test_one_trace_equals_per_frequency_traces(aircraft):

@@ -10,7 +10,9 @@ with a single-rank MPI stand-in (baseline/Makefile).  Checked here:
 * the engine's default mixed precision against the same USE_DOUBLE build:
   <= 0.1 dB on every sample within 30 dB of its frequency's strongest sample (the
   accuracy bar set for the engine), and the reference's own FP32 build reported
-  beside it.
+  beside it;
+* every sample, unfiltered: the mixed result within the error the engine states
+  for it against FP64 (sbr_error_bound) plus the engine-FP64 / reference-FP64 gap.
 """
 import numpy as np
 import pytest
@@ -59,9 +61,12 @@ def runs():
         job = sbr.JobSpec(r64["theta"], r64["phi"], fr, n, n, G, mb, 1.0)
         with sbr.Scene(v, t, device=0) as sc:
             e64 = sbr.run(sc, job, precision=sbr.PREC_FP64).sigma_m2
-            emx = sbr.run(sc, job, precision=sbr.PREC_MIXED).sigma_m2
+            mx = sbr.run(sc, job, precision=sbr.PREC_MIXED)
+            _, err_db = sbr.error_bound(sc, job, mx)
+        emx = mx.sigma_m2
         ref = r64["sigma"].T  # [angle, freq], the engine's order
-        out[name] = dict(ref64=ref, ref32=r32["sigma"].T, e64=e64.reshape(ref.shape), emx=emx.reshape(ref.shape))
+        out[name] = dict(ref64=ref, ref32=r32["sigma"].T, e64=e64.reshape(ref.shape), emx=emx.reshape(ref.shape),
+                         err_db=err_db.reshape(ref.shape))
     return out
 
 
@@ -82,3 +87,13 @@ def test_mixed_within_0p1_db_of_reference_double_build(runs, name):
     d32 = np.abs(_db(r["ref32"]) - d64)[lit]
     print(f"{name}: mixed max |d dB| {dmx.max():.3e}, reference FP32 build {d32.max():.3e} ({lit.sum()} samples)")
     assert dmx.max() <= 0.1, f"{name}: mixed max |d dB| {dmx.max():.3e} (reference FP32 build: {d32.max():.3e})"
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_mixed_unfiltered_within_stated_error(runs, name):
+    r = runs[name]
+    d64 = _db(r["ref64"])
+    dmx = np.abs(_db(r["emx"]) - d64)
+    gap = np.abs(_db(r["e64"]) - d64)
+    print(f"{name}: unfiltered mixed max |d dB| {dmx.max():.3e}, stated max {r['err_db'].max():.3e}")
+    assert np.all(dmx <= r["err_db"] + gap + 1e-9), (dmx.max(), r["err_db"].ravel()[np.argmax(dmx)])
