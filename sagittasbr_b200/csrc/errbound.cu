@@ -217,8 +217,12 @@ __device__ __forceinline__ void ray_bound(const ErrParams& P, const Segment& G, 
     float dnl = 0.0f;
     bool amb = false;
     for (int b = 0; b < J.max_bounces; ++b) {
-        const float m = 2.0f * (ue + ua * P.diag);
-        const float dt = 4.0f * m + 4.0f * kU * (norm1(r.o) + P.diag);
+        // a ray already bound for the FP64 re-trace needs no more margins: it walks
+        // unpadded (its uncertainty can grow to metres after a grazing bounce, and
+        // boxes widened that far would open most of the tree)
+        const bool exact = amb || 2.0 * kmax * dL > kPhaseExact;
+        const float m = exact ? 0.0f : 2.0f * (ue + ua * P.diag);
+        const float dt = exact ? 0.0f : 4.0f * m + 4.0f * kU * (norm1(r.o) + P.diag);
         float tB = 1e20f;
         const int slot = closest_flag(P.S, r.o, r.d, 1.0e-3f, tB, m, dt, amb, err);
         if (slot < 0) break;
