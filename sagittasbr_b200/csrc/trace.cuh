@@ -414,7 +414,16 @@ struct Walker<false> {
                 const int nh = int(h0) + int(h1) + int(h2) + int(h3);
                 if (nh == 1) {
                     ref = h0 ? c[0] : h1 ? c[1] : h2 ? c[2] : c[3];
-                } else if (nh > 1) {
+                } else if (nh == 2) {
+                    // the first and the last accepted child: enter the nearer, push the other
+                    const float ta = h0 ? t[0] : h1 ? t[1] : t[2];
+                    const int ca = h0 ? c[0] : h1 ? c[1] : c[2];
+                    const float tb = h3 ? t[3] : h2 ? t[2] : t[1];
+                    const int cb = h3 ? c[3] : h2 ? c[2] : c[1];
+                    const bool sw = tb < ta;
+                    push(sw ? ca : cb, sw ? ta : tb);
+                    ref = sw ? cb : ca;
+                } else if (nh > 2) {
                     const float inf = __int_as_float(0x7f800000);
                     t[0] = h0 ? t[0] : inf;
                     t[1] = h1 ? t[1] : inf;
