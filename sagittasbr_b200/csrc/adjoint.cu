@@ -59,15 +59,18 @@ __device__ __forceinline__ void scatter(double* g, uint32_t v, D3 a) {
     atomicAdd(g + 3 * v + 2, a.z);
 }
 
-// 1. The precision's own hit sequence of one ray per lane (called by all 32 lanes
-// of the warp; `valid` lanes hold a ray): caller triangle ids in rec.tri, the hit
-// count returned.  The walk takes one closest-hit query per step for the whole
-// warp, like the sweep kernel: without that synchronisation the lanes of a warp
-// drift apart on their own BVH paths and run nearly one at a time.
+// One ray per lane (called by all 32 lanes of the warp; `valid` lanes hold a ray):
+// frozen path, FP64 re-evaluation, reverse sweep.  Frequency adjoints are added to
+// the lane's own row gk[0..K).  The walk takes one closest-hit query per step for
+// the whole warp, like the sweep kernel: without that synchronisation the lanes of
+// a warp drift apart on their own BVH paths and run nearly one at a time.
 template <int PREC>
-__device__ __forceinline__ int walk_path(const AdjointParams& P, const Segment& G, const JobConst& J, int i, int j,
-                                         bool valid, sbr_ray_record& rec, uint32_t& err) {
+__device__ __forceinline__ void adjoint_ray(const AdjointParams& P, const Segment& G, const JobConst& J,
+                                            const FreqConst* F, int K, const double* cot, int i, int j, bool valid,
+                                            double* gk, uint32_t& err) {
     constexpr unsigned FULL = 0xffffffffu;
+    // 1. the precision's own hit sequence (caller triangle ids)
+    sbr_ray_record rec;
     int n = 0;
     bool walking = valid && J.max_bounces > 0;
     if (PREC == SBR_PREC_FP64) {
@@ -87,15 +90,8 @@ __device__ __forceinline__ int walk_path(const AdjointParams& P, const Segment& 
             if (walking) walking = !step_f<PREC, true, false>(r, e, P.S, J.max_bounces, err, &rec, nullptr);
         n = valid ? r.count : 0;
     }
-    return n;
-}
+    if (n == 0) return;
 
-// 2.-3. The frozen path of a ray that hit n > 0 triangles (caller ids tri[0..n)):
-// FP64 re-evaluation and reverse sweep.  Frequency adjoints are added to the lane's
-// own row gk[0..K).
-__device__ __forceinline__ void path_grad(const AdjointParams& P, const Segment& G, const JobConst& J,
-                                          const FreqConst* F, int K, const double* cot, int i, int j, int n,
-                                          const int32_t* tri_ids, double* gk) {
     // 2. FP64 forward along the frozen path
     double oS[kAdjMaxBounces][3], dS[kAdjMaxBounces][3], tS[kAdjMaxBounces];
     D3 o{G.llc[0] + (double(i) + 0.5) / double(J.nx) * G.u[0] + (double(j) + 0.5) / double(J.ny) * G.v[0],
@@ -105,7 +101,7 @@ __device__ __forceinline__ void path_grad(const AdjointParams& P, const Segment&
     double L = G.shift;
     D3 nLast{0, 0, 0}, dLast{0, 0, 0};
     for (int b = 0; b < n; ++b) {
-        const int tri = tri_ids[b];
+        const int tri = rec.tri[b];
         const D3 a = vertex(P, __ldg(P.idx + 3 * tri)), bb = vertex(P, __ldg(P.idx + 3 * tri + 1)),
                  c = vertex(P, __ldg(P.idx + 3 * tri + 2));
         const D3 N = cross(bb - a, c - a);
@@ -145,7 +141,7 @@ __device__ __forceinline__ void path_grad(const AdjointParams& P, const Segment&
     // 3. reverse sweep over the bounces
     D3 ob{0, 0, 0}, db{0, 0, 0};  // adjoints of the origin / direction after bounce b
     for (int b = n - 1; b >= 0; --b) {
-        const int tri = tri_ids[b];
+        const int tri = rec.tri[b];
         const uint32_t ia = __ldg(P.idx + 3 * tri), ib = __ldg(P.idx + 3 * tri + 1), ic = __ldg(P.idx + 3 * tri + 2);
         const D3 a = vertex(P, ia), e1 = vertex(P, ib) - a, e2 = vertex(P, ic) - a;
         const D3 N = cross(e1, e2);
@@ -192,24 +188,13 @@ __device__ __forceinline__ void path_grad(const AdjointParams& P, const Segment&
     }
 }
 
-// A hit ray's frozen path, queued per warp in shared memory: the FP64 phases run
-// only on full warps of hit rays (rays that miss take no part), instead of on the
-// lanes of each 4x8 block that happened to hit.
-struct PathEntry {
-    int32_t i, j, n;
-    int32_t tri[kAdjMaxBounces];
-};
-constexpr int kPathQueue = 64;  // up to 31 waiting + one block of 32
-
 // 6 resident CTAs per SM (80 registers): measured 8 % faster on B200 than the
 // unconstrained 128-register build despite the spills.
 template <int PREC>
 __global__ void __launch_bounds__(kCtaThreads, 6) k_adjoint(const AdjointParams P) {
     constexpr unsigned FULL = 0xffffffffu;
-    __shared__ PathEntry s_paths[kCtaThreads / 32][kPathQueue];
     double gk[kAdjMaxK];  // this lane's dLoss/dk of the current item (local memory)
     const int lane = threadIdx.x & 31;
-    PathEntry* const q = s_paths[threadIdx.x >> 5];
     uint32_t err = 0;
     int iter = 0;
     for (;;) {
@@ -233,36 +218,13 @@ __global__ void __launch_bounds__(kCtaThreads, 6) k_adjoint(const AdjointParams 
         for (int k = 0; k < K; ++k) gk[k] = 0.0;
         const int b0 = int(item - G.item_base) * G.blocks_per_item;
         const int nslots = min(G.blocks_per_item, G.blocks - b0) * 32;
-        int queued = 0;  // warp-uniform
         for (int s0 = 0; s0 < nslots; s0 += 32) {  // one 4x8 ray block per step, all lanes
             const int s = s0 + lane;
             const int blk = b0 + (s >> 5), l = s & 31;
             const int i = G.i0 + (blk % G.blocks_x) * kBlockW + (l % kBlockW);
             const int j = G.j0 + (blk / G.blocks_x) * kBlockH + (l / kBlockW);
-            sbr_ray_record rec;
-            const int n = walk_path<PREC>(P, G, J, i, j, i < G.i0 + G.ni && j < G.j0 + G.nj, rec, err);
-            const unsigned hit = __ballot_sync(FULL, n > 0);
-            if (n > 0) {
-                PathEntry& e = q[queued + __popc(hit & ((1u << lane) - 1u))];
-                e.i = i;
-                e.j = j;
-                e.n = n;
-                for (int b = 0; b < n; ++b) e.tri[b] = rec.tri[b];
-            }
-            queued += __popc(hit);
-            __syncwarp();
-            if (queued >= 32) {  // a full warp of hit rays: the top 32 entries
-                const PathEntry& e = q[queued - 32 + lane];
-                path_grad(P, G, J, F, K, cot, e.i, e.j, e.n, e.tri, gk);
-                __syncwarp();
-                queued -= 32;
-            }
+            adjoint_ray<PREC>(P, G, J, F, K, cot, i, j, i < G.i0 + G.ni && j < G.j0 + G.nj, gk, err);
         }
-        if (lane < queued) {
-            const PathEntry& e = q[lane];
-            path_grad(P, G, J, F, K, cot, e.i, e.j, e.n, e.tri, gk);
-        }
-        __syncwarp();
         // lanes -> warp in a fixed order, one atomic per (item, frequency)
         for (int k = 0; k < K; ++k) {
             double v = gk[k];
