@@ -323,9 +323,12 @@ def oracle_counts(w, n_angles: int = 8, per_angle: int = 512, threads: int = 0):
 
 
 # DRAM bytes per closest-hit query of k_trace, from one ncu capture per workload
-# (dram__bytes_read.sum + dram__bytes_write.sum of one launch / the queries of that
-# launch), scaled by the queries of a full launch.
-DRAM_BYTES_PER_QUERY = {}
+# (dram__bytes_read.sum + dram__bytes_write.sum of one launch / the closest-hit
+# queries of that launch), scaled by the queries of a full launch:
+#   aircraft: 8 of the 721 azimuths, 64 frequencies, one launch: 709.2 MB read +
+#             144.0 MB written for 4.253e8 queries;
+#   trihedral: 64 of the 8,281 angles, one launch: 4.82 MB + 1.25 MB for 2.96e7 queries.
+DRAM_BYTES_PER_QUERY = {"aircraft": 2.006, "trihedral": 0.205}
 
 
 def hbm_peak_gbs() -> tuple[float, str]:
