@@ -221,24 +221,34 @@ class Clocks:
 
 
 def fp32_peak_tflops(torch) -> float:
-    """Dense FP32 (no TF32) SGEMM throughput, best of 5 at 8192^3."""
+    """Dense FP32 (no TF32) SGEMM throughput at 8192^3: after a second of warm-up
+    GEMMs, the best of 10 bursts of three back-to-back GEMMs."""
     torch.backends.cuda.matmul.allow_tf32 = False
     n = 8192
     a = torch.randn(n, n, device="cuda")
     b = torch.randn(n, n, device="cuda")
-    for _ in range(2):
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < 1.0:
         a @ b
-    torch.cuda.synchronize()
+        torch.cuda.synchronize()
     best = 0.0
-    for _ in range(5):
+    for _ in range(10):
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s.record()
-        a @ b
+        for _ in range(3):
+            a @ b
         e.record()
         e.synchronize()
-        best = max(best, 2 * n ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+        best = max(best, 3 * 2 * n ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
     del a, b
     return best
+
+
+def fma_peak_tflops(torch, sm_mhz: float) -> float:
+    """The FP32 FMA issue rate of the device at a given SM clock: SMs x 128 FP32
+    lanes x 2 FLOP per cycle."""
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    return sms * 128 * 2 * sm_mhz * 1e6 / 1e12
 
 
 def config_of(w) -> dict:
@@ -792,6 +802,7 @@ def main():
                 "kernel": "k_trace (persistent) + k_finalize", "flop_per_query": flop_q, "v_box": vbox, "v_tri": vtri,
                 "queries_per_launch": queries_all / ws, "counts": counts,
                 "peak_source": "FP32 SGEMM 8192^3 measured in this run, per GPU (no FP32 figure in the peaks file)",
+                "fp32_fma_rate_at_sampled_clock": (fma_peak_tflops(torch, clk["sm_mhz"]) if clk else None),
                 "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum per query of a subset capture, "
                                    "x queries of a full launch") if dq is not None else None,
                 "hbm_view": {"bytes_per_query": 48 * (vbox + vtri),
