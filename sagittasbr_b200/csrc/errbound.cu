@@ -22,18 +22,20 @@
 // (boxes only prune; the closest hit does not change).  For those rays the exact
 // difference of the FP64 and mixed terms is summed per sample (Delta_k).  The other
 // rays differ from FP64 only by rounding, |d term| <= scale_k (amp 2 k dL + amp eps
-// + damp), damp = 2 R^n (dn_last + a).  Those rounding errors are partly shared by
-// many rays (a face-on plate: every ray has nearly the same path and the same
-// rounding) and partly independent.  The shared part is bounded by the mean per-ray
-// bound times the field itself (c1 = sum amp dL / sum amp, c0 = sum (amp eps +
-// damp) / sum amp); the rest, taken as fully correlated within a work item (up to
-// 256 neighbouring rays) and independent between items, by the probabilistic
-// rounding-error bound of Higham and Mary (SIAM J. Sci. Comput. 41(5), 2019):
-// |sum| <= lambda sqrt(sum of squares), exceeded with probability below
+// + damp), damp = 2 R^n (dn_last + a).  Part of those errors is the same for every
+// ray that sees the same geometry the same way (a face-on plate): the relative error
+// of t from the approximate reciprocals of the triangle test (bounded by 8 u t per
+// bounce, dLs) and the error of the sine / cosine approximation (eps).  That shared
+// part adds coherently, so it is bounded by the field itself times its
+// amp-weighted mean, |S_k| (2 k c1 + eps) with c1 = sum amp dLs / sum amp.  The rest
+// varies from ray to ray; taken as fully correlated within a work item (up to 256
+// neighbouring rays) and independent between items, it is bounded with the
+// probabilistic rounding-error bound of Higham and Mary (SIAM J. Sci. Comput. 41(5),
+// 2019): |sum| <= lambda sqrt(sum of squares), exceeded with probability below
 // 4 exp(-lambda^2 / 2) (lambda = 6: 6e-8).  Per sample
-//   E_k = |Delta_k| + |S_k| (2 k c1 + c0) + lambda scale_k (2 k sqrt(Q1) + sqrt(Q0))
+//   E_k = |Delta_k| + |S_k| (2 k c1 + eps) + lambda scale_k (2 k sqrt(Q1) + sqrt(Q0))
 //         + (items + 1) quantum_k,
-// Q1 = sum over items of (sum amp dL)^2, Q0 likewise for amp eps + damp, over the
+// Q1 = sum over items of (sum amp dL)^2, Q0 likewise for damp, over the
 // rounding-only rays; the last term covers the fixed-point fold of the sweep.
 #include <algorithm>
 #include <cmath>
@@ -62,7 +64,7 @@ struct ErrParams {
     const FreqConst* freqs;
     int64_t n_items;
     unsigned long long* queue;
-    double* acc;       // [n_segs][8]: sum amp, sum amp dL, sum a0, Q1, Q0, re-traced rays, rays, -
+    double* acc;       // [n_segs][8]: sum amp, sum amp dLs, -, Q1, Q0, re-traced rays, rays, -
     double* dfield;    // [n_samples][2]: sum of (FP64 term - mixed term) of the re-traced rays
     float diag;        // scene bounding-box diagonal (m)
     uint32_t* err;
@@ -213,13 +215,14 @@ __device__ int closest_flag(const SceneView& S, F3 o, F3 d, float tMin, float& t
 // phase uncertainty are re-traced with the FP64 sweep's own step and their term
 // differences added to dfield, the others add to the lane's sums of squares.
 __device__ __forceinline__ void ray_bound(const ErrParams& P, const Segment& G, const JobConst& J, const FreqConst* F,
-                                         int K, double kmax, int i, int j, double& sa, double& s1, double& s0,
-                                         unsigned& nex, uint32_t& err) {
+                                         int K, double kmax, int i, int j, double& sa, double& s1, double& q1,
+                                         double& s0, unsigned& nex, uint32_t& err) {
     RayF r;
     start_f<SBR_PREC_MIXED>(r, G, J, i, j);
     float ue = 2.0f * kU * norm1(r.o);  // origin formed in FP64, rounded to FP32
     float ua = 2.0f * kU;                // FP32 direction
     double dL = double(kU * norm1(r.o));
+    double dLs = 0.0;  // the part shared by rays seeing the same geometry the same way
     float dnl = 0.0f;
     bool amb = false;
     for (int b = 0; b < J.max_bounces; ++b) {
@@ -251,8 +254,9 @@ __device__ __forceinline__ void ray_bound(const ErrParams& P, const Segment& G, 
         const float sinang = sqrtf(dot(N, N) / fmaxf(dot(e1, e1) * dot(e2, e2), 1e-30f));
         const float dnrm = 8.0f * kU / fmaxf(sinang, 1e-6f);
         const float ci = fmaxf(fabsf(r.cosl), 1e-6f);
-        const float dtb = (ue + tB * ua) / ci + 4.0f * kU * tB;
+        const float dtb = (ue + tB * ua) / ci + 8.0f * kU * tB;
         dL += double(dtb);
+        dLs += double(8.0f * kU * tB);
         ue = ue + tB * ua + dtb + 2.0f * kU * norm1(p) + 1.0e-4f * dnrm;
         ua = ua + 2.0f * dnrm + 4.0f * kU;
         dnl = dnrm;
@@ -282,8 +286,9 @@ __device__ __forceinline__ void ray_bound(const ErrParams& P, const Segment& G, 
         ++nex;
     } else if (r.count > 0) {
         sa += double(om.amp);
-        s1 += double(om.amp) * dL;
-        s0 += double(om.amp) * kPhaseEps + 2.0 * double(fabsf(om.Rn)) * double(dnl + ua);
+        s1 += double(om.amp) * dLs;
+        q1 += double(om.amp) * dL;
+        s0 += 2.0 * double(fabsf(om.Rn)) * double(dnl + ua);
     }
 }
 
@@ -310,19 +315,20 @@ __global__ void __launch_bounds__(kCtaThreads) k_errbound(const ErrParams P) {
         for (int k = 0; k < J.n_freqs; ++k) kmax = fmax(kmax, F[k].k);
         const int b0 = int(item - G.item_base) * G.blocks_per_item;
         const int b1 = min(b0 + G.blocks_per_item, G.blocks);
-        double sa = 0.0, s1 = 0.0, s0 = 0.0;
+        double sa = 0.0, s1 = 0.0, q1 = 0.0, s0 = 0.0;
         unsigned nex = 0, nray = 0;
         for (int blk = b0; blk < b1; ++blk) {
             const int i = G.i0 + (blk % G.blocks_x) * kBlockW + (lane % kBlockW);
             const int j = G.j0 + (blk / G.blocks_x) * kBlockH + (lane / kBlockW);
             if (i < G.i0 + G.ni && j < G.j0 + G.nj) {
-                ray_bound(P, G, J, F, J.n_freqs, kmax, i, j, sa, s1, s0, nex, err);
+                ray_bound(P, G, J, F, J.n_freqs, kmax, i, j, sa, s1, q1, s0, nex, err);
                 ++nray;
             }
         }
         for (int off = 16; off > 0; off >>= 1) {
             sa += __shfl_xor_sync(FULL, sa, off);
             s1 += __shfl_xor_sync(FULL, s1, off);
+            q1 += __shfl_xor_sync(FULL, q1, off);
             s0 += __shfl_xor_sync(FULL, s0, off);
         }
         nex = __reduce_add_sync(FULL, nex);
@@ -331,8 +337,7 @@ __global__ void __launch_bounds__(kCtaThreads) k_errbound(const ErrParams P) {
             double* A = P.acc + 8 * seg;
             atomicAdd(A, sa);
             atomicAdd(A + 1, s1);
-            atomicAdd(A + 2, s0);
-            atomicAdd(A + 3, s1 * s1);  // the item's rounding errors taken as fully correlated
+            atomicAdd(A + 3, q1 * q1);  // the item's rounding errors taken as fully correlated
             atomicAdd(A + 4, s0 * s0);
             atomicAdd(A + 5, double(nex));
             atomicAdd(A + 6, double(nray));
@@ -434,7 +439,7 @@ extern "C" sbr_status sbr_error_bound(sbr_scene* s, const sbr_job* jobs, size_t 
                 const int64_t smp = G.sample_base + k;
                 const double* A = acc.data() + 8 * g;
                 const double a = std::hypot(field[2 * smp], field[2 * smp + 1]);
-                const double shared = A[0] > 0.0 ? a * (2.0 * F.k * A[1] + A[2]) / A[0] : 0.0;
+                const double shared = a * ((A[0] > 0.0 ? 2.0 * F.k * A[1] / A[0] : 0.0) + kPhaseEps);
                 const double E = std::hypot(dfield[2 * smp], dfield[2 * smp + 1]) + shared +
                                  kLambda * F.scale * (2.0 * F.k * std::sqrt(A[3]) + std::sqrt(A[4])) +
                                  double(items + 1) * F.quantum;
