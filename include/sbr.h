@@ -234,10 +234,12 @@ sbr_status sbr_run(sbr_scene* scene, const sbr_job* jobs, size_t n_jobs, sbr_res
  * edge within reach of the ray, |det| near its 1e-6 threshold, t near tMin or tied
  * with another hit) or whose phase uncertainty exceeds 0.05 rad are re-traced with
  * the FP64 sweep's own arithmetic and their exact difference is summed; the other
- * rays differ by rounding only: the part of those errors shared by many rays is
- * bounded by their mean bound times |field|, the rest (correlated within a work
- * item of up to 256 neighbouring rays, independent between items) by a
- * probabilistic rounding-error bound exceeded with probability below 6e-8.
+ * rays differ by rounding only: the part of those errors that is the same for all
+ * rays seeing the same geometry the same way (the systematic rounding of the hit
+ * distance, the sine / cosine approximation) is bounded coherently, as a fraction
+ * of |field|, the rest (correlated within a work item of up to 256 neighbouring
+ * rays, independent between items) by a probabilistic rounding-error bound
+ * exceeded with probability below 6e-8.
  *   field     [n_samples * 2] in: the mixed-precision fields sbr_run returned.
  *   err_field [n_samples] out (may be NULL): stated |field - field_FP64|.
  *   err_db    [n_samples] out (may be NULL): the |dBsm - dBsm_FP64| it implies (dBsm
