@@ -70,7 +70,10 @@ inline int pick_epi(int channels) {
 // 8 -> 64 registers per thread, 32 warps per SM.  The walk is latency-bound (node
 // loads from L1/L2), so more resident warps beat fewer spills: measured on B200,
 // 6 / 7 / 8 CTAs gave 41.2k / 43.2k / 44.9k trihedral samples/s.
-constexpr int kMinCtasPerSm = 8;
+#ifndef SBR_TRACE_CTAS_PER_SM
+#define SBR_TRACE_CTAS_PER_SM 8
+#endif
+constexpr int kMinCtasPerSm = SBR_TRACE_CTAS_PER_SM;
 
 // Polarised exit terms of a finished ray (SBR_POL_HHVV): the HH and VV amplitudes
 // and the physical exit path L + (plane - s.p_last), i.e. the path from the launch
