@@ -254,14 +254,4 @@ __device__ __forceinline__ void po_term(int prec, const FreqConst& F, const RayO
     }
 }
 
-// The MIXED branch of po_term with the channel's k / pi already in a register:
-// the same operations in the same order.
-__device__ __forceinline__ void po_term_mixed(double turns, float amp, double L, double& re, double& im) {
-    float s, c;
-    sincos_turns(turns * L, s, c);
-    const double a = double(amp);
-    re -= a * double(s);
-    im += a * double(c);
-}
-
 }  // namespace sbr

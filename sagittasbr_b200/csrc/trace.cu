@@ -191,17 +191,6 @@ __global__ void __launch_bounds__(kCtaThreads, kMinCtasPerSm) k_trace(const Trac
         const int i_end = G.i0 + G.ni, j_end = G.j0 + G.nj;
         const int KC = K * NPOL;  // channels of this item
 
-        // mixed scalar sweeps: the phase scale k / pi of the channels this lane adds
-        // to, loaded once per item instead of once per finished ray
-        constexpr bool MXS = PREC == SBR_PREC_MIXED && !POL;
-        double turnsC[MXS ? NACC : 1];
-        if constexpr (MXS) {
-#pragma unroll
-            for (int c = 0; c < NACC; ++c) {
-                const int ch = TRANSPOSED ? c * 32 + lane : c;
-                turnsC[c] = ch < KC ? F[ch].turns : 0.0;
-            }
-        }
         double accRe[SACC ? 1 : NACC], accIm[SACC ? 1 : NACC];
 #pragma unroll
         for (int c = 0; c < NACC; ++c) {
@@ -291,7 +280,6 @@ __global__ void __launch_bounds__(kCtaThreads, kMinCtasPerSm) k_trace(const Trac
                     for (int ch = 0; ch < NACC; ++ch) {
                         if (ch < KC) {
                             if constexpr (POL) po_term_pol(PREC, F[ch >> 1], out.Lp, out.pa[ch & 1], accRe[ch], accIm[ch]);
-                            else if constexpr (MXS) po_term_mixed(turnsC[ch], out.amp, out.L, accRe[ch], accIm[ch]);
                             else po_term(PREC, F[ch], out, accRe[ch], accIm[ch]);
                         }
                     }
@@ -308,9 +296,6 @@ __global__ void __launch_bounds__(kCtaThreads, kMinCtasPerSm) k_trace(const Trac
                         q.pa[0] = __shfl_sync(FULL, out.pa[0], src);
                         q.pa[1] = __shfl_sync(FULL, out.pa[1], src);
                         q.Lp = __shfl_sync(FULL, out.Lp, src);
-                    } else if constexpr (MXS) {  // the mixed term reads amp and L only
-                        q.amp = __shfl_sync(FULL, out.amp, src);
-                        q.L = __shfl_sync(FULL, out.L, src);
                     } else {
                         q.amp = __shfl_sync(FULL, out.amp, src);
                         q.L = __shfl_sync(FULL, out.L, src);
@@ -326,7 +311,6 @@ __global__ void __launch_bounds__(kCtaThreads, kMinCtasPerSm) k_trace(const Trac
                         if (ch < KC) {
                             if constexpr (SACC) po_term_pol(PREC, F[ch >> 1], q.Lp, q.pa[ch & 1], my_acc[c * 32].x, my_acc[c * 32].y);
                             else if constexpr (POL) po_term_pol(PREC, F[ch >> 1], q.Lp, q.pa[ch & 1], accRe[c], accIm[c]);
-                            else if constexpr (MXS) po_term_mixed(turnsC[c], q.amp, q.L, accRe[c], accIm[c]);
                             else po_term(PREC, F[ch], q, accRe[c], accIm[c]);
                         }
                     }
