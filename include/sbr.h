@@ -237,9 +237,8 @@ sbr_status sbr_run(sbr_scene* scene, const sbr_job* jobs, size_t n_jobs, sbr_res
  * rays differ by rounding only: the part of those errors that is the same for all
  * rays seeing the same geometry the same way (the systematic rounding of the hit
  * distance, the sine / cosine approximation) is bounded coherently, as a fraction
- * of |field|, the rest (correlated within a work item of up to 256 neighbouring
- * rays, independent between items) by a probabilistic rounding-error bound
- * exceeded with probability below 6e-8.
+ * of |field|, the rest (independent from ray to ray) by a probabilistic
+ * rounding-error bound exceeded with probability below 6e-8.
  *   field     [n_samples * 2] in: the mixed-precision fields sbr_run returned.
  *   err_field [n_samples] out (may be NULL): stated |field - field_FP64|.
  *   err_db    [n_samples] out (may be NULL): the |dBsm - dBsm_FP64| it implies (dBsm

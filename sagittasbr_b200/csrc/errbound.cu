@@ -28,15 +28,15 @@
 // bounce, dLs) and the error of the sine / cosine approximation (eps).  That shared
 // part adds coherently, so it is bounded by the field itself times its
 // amp-weighted mean, |S_k| (2 k c1 + eps) with c1 = sum amp dLs / sum amp.  The rest
-// varies from ray to ray; taken as fully correlated within a work item (up to 256
-// neighbouring rays) and independent between items, it is bounded with the
-// probabilistic rounding-error bound of Higham and Mary (SIAM J. Sci. Comput. 41(5),
-// 2019): |sum| <= lambda sqrt(sum of squares), exceeded with probability below
-// 4 exp(-lambda^2 / 2) (lambda = 6: 6e-8).  Per sample
+// (origin, hit-point and direction rounding) varies from ray to ray as independent,
+// zero-mean errors, bounded with the probabilistic rounding-error bound of Higham
+// and Mary (SIAM J. Sci. Comput. 41(5), 2019): |sum| <= lambda sqrt(sum of squares),
+// exceeded with probability below 4 exp(-lambda^2 / 2) (lambda = 6: 6e-8).  Per
+// sample
 //   E_k = |Delta_k| + |S_k| (2 k c1 + eps) + lambda scale_k (2 k sqrt(Q1) + sqrt(Q0))
 //         + (items + 1) quantum_k,
-// Q1 = sum over items of (sum amp dL)^2, Q0 likewise for damp, over the
-// rounding-only rays; the last term covers the fixed-point fold of the sweep.
+// Q1 = sum (amp (dL - dLs))^2, Q0 = sum damp^2 over the rounding-only rays; the
+// last term covers the fixed-point fold of the sweep.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -287,8 +287,9 @@ __device__ __forceinline__ void ray_bound(const ErrParams& P, const Segment& G, 
     } else if (r.count > 0) {
         sa += double(om.amp);
         s1 += double(om.amp) * dLs;
-        q1 += double(om.amp) * dL;
-        s0 += 2.0 * double(fabsf(om.Rn)) * double(dnl + ua);
+        const double e1 = double(om.amp) * (dL - dLs), e0 = 2.0 * double(fabsf(om.Rn)) * double(dnl + ua);
+        q1 += e1 * e1;
+        s0 += e0 * e0;
     }
 }
 
@@ -337,8 +338,8 @@ __global__ void __launch_bounds__(kCtaThreads) k_errbound(const ErrParams P) {
             double* A = P.acc + 8 * seg;
             atomicAdd(A, sa);
             atomicAdd(A + 1, s1);
-            atomicAdd(A + 3, q1 * q1);  // the item's rounding errors taken as fully correlated
-            atomicAdd(A + 4, s0 * s0);
+            atomicAdd(A + 3, q1);  // sums of squares of independent per-ray bounds
+            atomicAdd(A + 4, s0);
             atomicAdd(A + 5, double(nex));
             atomicAdd(A + 6, double(nray));
         }
