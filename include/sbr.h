@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define SBR_ABI_VERSION 2  /* 2: sbr_config.error_bound, sbr_build_opts.node_width */
+#define SBR_ABI_VERSION 2  /* 2: sbr_config.error_bound, sbr_build_opts / sbr_run_opts / sbr_plan_info.node_width */
 
 /* ------------------------------------------------------------------ status */
 typedef int32_t sbr_status;
@@ -166,9 +166,12 @@ typedef struct sbr_run_opts {
     int32_t blocks_per_item;  /* 32-ray blocks (4 x 8) per work item; 0 -> automatic (batched: blocks / 1024
                                  clamped to 1..8 per angle, per-angle mode: 1) */
     int32_t autotune;         /* 1: sbr_plan_create times candidate (blocks_per_item, ctas_per_sm)
-                                 settings on a sample of the plan's angles and keeps the fastest
+                                 settings -- and both tree widths when the scene holds an 8-wide
+                                 tree -- on a sample of the plan's angles and keeps the fastest
                                  (batched mode; adds about 20 short launches to plan creation) */
-    int32_t reserved[4];
+    int32_t node_width;       /* tree the mixed-precision scalar sweep walks: 0 -> the scene's widest
+                                 (8 when built with sbr_build_opts.node_width = 8), 4, or 8 */
+    int32_t reserved[3];
 } sbr_run_opts;
 
 /* Results for every (job, angle, frequency[, polarization]) in job order, then
@@ -198,6 +201,7 @@ typedef struct sbr_plan_info {
     int64_t d2h_bytes;        /* bytes sbr_plan_results copies device -> host (field, stats, error word) */
     int32_t blocks_per_item;  /* the plan's setting (0: automatic per angle) */
     int32_t ctas_per_sm;      /* persistent CTAs per SM of the trace launches */
+    int32_t node_width;       /* tree width the plan's mixed scalar sweep walks (4 or 8) */
 } sbr_plan_info;
 
 sbr_status sbr_plan_create(sbr_scene* scene, const sbr_job* jobs, size_t n_jobs, const sbr_run_opts* opts,

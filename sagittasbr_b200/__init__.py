@@ -163,7 +163,7 @@ class SweepResult:
 
 
 def _opts(mode, precision, polarization=POL_SCALAR, stream=None, use_graph=False, ctas_per_sm=0,
-          first_hit=FIRST_HIT_TRAVERSE, blocks_per_item=0, autotune=False):
+          first_hit=FIRST_HIT_TRAVERSE, blocks_per_item=0, autotune=False, node_width=0):
     o = _lib.RunOpts()
     o.mode, o.precision, o.polarization = int(mode), int(precision), int(polarization)
     o.use_graph = 1 if use_graph else 0
@@ -172,6 +172,7 @@ def _opts(mode, precision, polarization=POL_SCALAR, stream=None, use_graph=False
     o.first_hit = int(first_hit)
     o.blocks_per_item = int(blocks_per_item)
     o.autotune = 1 if autotune else 0
+    o.node_width = int(node_width)
     return o
 
 
@@ -188,7 +189,7 @@ class Plan:
     def __init__(self, scene: Scene | Sequence[Scene], jobs: Sequence[JobSpec], mode=MODE_BATCHED,
                  precision=PREC_MIXED, stream=None, use_graph=False, ctas_per_sm=0, first_hit=None,
                  polarization=POL_SCALAR, job_scene: Sequence[int] | None = None, blocks_per_item=0,
-                 autotune=False):
+                 autotune=False, node_width=0):
         """With a list of scenes, job j traces scene[job_scene[j]] (sbr_plan_create_multi).
         autotune=True times candidate (blocks_per_item, ctas_per_sm) settings on a sample of
         the angles first and keeps the fastest (batched mode); info reports the choice."""
@@ -197,7 +198,7 @@ class Plan:
         self._jc = _jobs_c(self.jobs)
         o = _opts(mode, precision, polarization, stream=stream, use_graph=use_graph, ctas_per_sm=ctas_per_sm,
                   first_hit=FIRST_HIT_TRAVERSE if first_hit is None else first_hit,
-                  blocks_per_item=blocks_per_item, autotune=autotune)
+                  blocks_per_item=blocks_per_item, autotune=autotune, node_width=node_width)
         h = C.c_void_p()
         if isinstance(scene, Scene):
             check(lib().sbr_plan_create(scene.handle, self._jc, len(self.jobs), C.byref(o), C.byref(h)),

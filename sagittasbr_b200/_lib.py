@@ -76,7 +76,8 @@ class RunOpts(C.Structure):
         ("first_hit", C.c_int32),
         ("blocks_per_item", C.c_int32),
         ("autotune", C.c_int32),
-        ("reserved", C.c_int32 * 4),
+        ("node_width", C.c_int32),
+        ("reserved", C.c_int32 * 3),
     ]
 
 
@@ -104,6 +105,7 @@ class PlanInfo(C.Structure):
         ("d2h_bytes", C.c_int64),
         ("blocks_per_item", C.c_int32),
         ("ctas_per_sm", C.c_int32),
+        ("node_width", C.c_int32),
     ]
 
 

@@ -334,8 +334,12 @@ sbr_status autotune(sbr_scene* const* scenes, size_t n_scenes, const int32_t* jo
     }
     const int bpis[] = {0, 1, 2, 4, 8, 16};
     const int ctas[] = {0, 6};
+    // both tree widths when a single-scene plan's scene holds an 8-wide tree
+    std::vector<int> widths{o.node_width};
+    if (!job_scene && o.node_width == 0 && scenes[0]->d_nodes8) widths = {4, 8};
     double best = INFINITY;
-    int best_bpi = 0, best_ctas = 0;
+    int best_bpi = 0, best_ctas = 0, best_w = o.node_width;
+    for (int w : widths)
     for (int c : ctas) {
         for (int b : bpis) {
             sbr_run_opts t = o;
@@ -343,6 +347,7 @@ sbr_status autotune(sbr_scene* const* scenes, size_t n_scenes, const int32_t* jo
             t.use_graph = 0;
             t.blocks_per_item = b;
             t.ctas_per_sm = c;
+            t.node_width = w;
             sbr_plan* pl = nullptr;
             sbr_status st = plan_create(scenes, n_scenes, job_scene, sj.data(), n_jobs, &t, &pl);
             if (st != SBR_OK) return st;
@@ -357,11 +362,13 @@ sbr_status autotune(sbr_scene* const* scenes, size_t n_scenes, const int32_t* jo
                 best = r.device_ms;
                 best_bpi = b;
                 best_ctas = c;
+                best_w = w;
             }
         }
     }
     o.blocks_per_item = best_bpi;
     o.ctas_per_sm = best_ctas;
+    o.node_width = best_w;
     return SBR_OK;
 }
 
@@ -377,6 +384,10 @@ sbr_status plan_create(sbr_scene* const* scenes, size_t n_scenes, const int32_t*
     sbr_status vs = validate_run(s, jobs, n_jobs, o);
     if (vs != SBR_OK) return vs;
     if (o.blocks_per_item < 0 || o.ctas_per_sm < 0) return fail(SBR_ERR_INVALID_ARG, "negative tuning option");
+    if (o.node_width != 0 && o.node_width != 4 && o.node_width != 8)
+        return fail(SBR_ERR_INVALID_ARG, "node_width must be 0, 4 or 8");
+    if (o.node_width == 8 && !s->d_nodes8)
+        return fail(SBR_ERR_UNSUPPORTED, "node_width 8 needs a scene built with sbr_build_opts.node_width = 8");
     for (size_t k = 0; k < n_scenes; ++k) {
         if (!scenes[k]) return fail(SBR_ERR_INVALID_ARG, "null scene");
         if (scenes[k]->device != s->device) return fail(SBR_ERR_INVALID_ARG, "scenes of one plan share a device");
@@ -413,6 +424,8 @@ sbr_status plan_create(sbr_scene* const* scenes, size_t n_scenes, const int32_t*
     p->num_sms = s->num_sms;
     p->stream = o.stream ? (cudaStream_t)o.stream : s->stream;
     p->scene_view = s->view();
+    p->node_width = !job_scene && ((o.node_width == 0 && s->d_nodes8) || o.node_width == 8) ? 8 : 4;
+    if (p->node_width == 4) p->scene_view.nodes8 = nullptr;  // the sweep kernel walks the 4-wide tree
     p->d_err = s->d_err;
     p->d_cancel = s->d_cancel;
 
@@ -599,6 +612,7 @@ sbr_status sbr_plan_info_get(const sbr_plan* p, sbr_plan_info* out) {
     out->n_pol = p->n_pol;
     out->blocks_per_item = p->blocks_per_item;
     out->ctas_per_sm = p->ctas_per_sm;
+    out->node_width = p->node_width;
     int64_t launches = 1;
     if (p->mode == SBR_MODE_BATCHED && p->raster) {
         for (const auto& ch : p->chunks) launches += 1 + (ch.item_end > ch.item_begin ? 1 : 0);

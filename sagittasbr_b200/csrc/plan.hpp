@@ -56,6 +56,7 @@ struct sbr_plan {
     int use_graph = 0;
     int ctas_per_sm = 0;
     int blocks_per_item = 0;
+    int node_width = 4;                      // tree the mixed scalar sweep walks
     int num_sms = 0;
     cudaStream_t stream = nullptr;
     sbr::SceneView scene_view{};

@@ -56,3 +56,23 @@ def test_node_width_validation_and_refit_drops_the_wide_tree():
         s8.update_vertices(v2)
         s4.update_vertices(v2)
         np.testing.assert_array_equal(sbr.run(s8, job).field, sbr.run(s4, job).field)
+
+
+def test_plan_node_width_and_autotuned_width():
+    """A plan walks the scene's widest tree by default, the 4-wide one on request,
+    and the autotuner times both widths when the scene holds an 8-wide tree."""
+    v, t = M.trihedral(1.0, 20)
+    th, ph = np.meshgrid(np.linspace(5, 85, 5), np.linspace(5, 85, 5), indexing="ij")
+    job = sbr.JobSpec(th.ravel(), ph.ravel(), [1e10], 160, 160, 2.0 * M.bounding_radius(v), 3)
+    with sbr.Scene(v, t, node_width=8) as s8, sbr.Scene(v, t) as s4:
+        ref = sbr.run(s4, job).field
+        for kw, want in (({}, 8), ({"node_width": 4}, 4), ({"node_width": 8}, 8), ({"autotune": True}, None)):
+            pl = sbr.Plan(s8, [job], **kw)
+            assert pl.info["node_width"] == (want if want else pl.info["node_width"])
+            assert pl.info["node_width"] in (4, 8)
+            pl.execute()
+            np.testing.assert_array_equal(pl.results().field, ref)
+            pl.close()
+        assert sbr.Plan(s4, [job]).info["node_width"] == 4
+        with pytest.raises(sbr.SbrError):
+            sbr.Plan(s4, [job], node_width=8)
