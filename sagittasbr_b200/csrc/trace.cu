@@ -66,14 +66,19 @@ struct Epi {
 inline int pick_epi(int channels) {
     return channels <= 1 ? EPI_LANE1 : channels <= kRegK ? EPI_LANE4 : channels <= 64 ? EPI_T64 : EPI_T128;
 }
-// Resident CTAs (of 4 warps) per SM the kernels are register-budgeted for:
-// 8 -> 64 registers per thread, 32 warps per SM.  The walk is latency-bound (node
-// loads from L1/L2), so more resident warps beat fewer spills: measured on B200,
-// 6 / 7 / 8 CTAs gave 41.2k / 43.2k / 44.9k trihedral samples/s.
+// Resident CTAs (of 4 warps) per SM the kernels are register-budgeted for, by
+// epilogue layout: the walk is latency-bound (node loads from L1/L2), so resident
+// warps matter, but the wide layouts hold more state.  Measured on B200: per-lane
+// layouts, trihedral (1 channel) 50,993 / 49,455 / 47,565 samples/s at 8 / 7 / 6
+// CTAs (64 / 72 / 80 registers); lane-owned layouts, aircraft (64 channels)
+// 13,180 / 13,499 / 12,948.  SBR_TRACE_CTAS_PER_SM (build flag) overrides both.
 #ifndef SBR_TRACE_CTAS_PER_SM
-#define SBR_TRACE_CTAS_PER_SM 8
+#define SBR_TRACE_CTAS_PER_SM 0
 #endif
-constexpr int kMinCtasPerSm = SBR_TRACE_CTAS_PER_SM;
+template <int EPI>
+constexpr int min_ctas_per_sm() {
+    return SBR_TRACE_CTAS_PER_SM > 0 ? SBR_TRACE_CTAS_PER_SM : (EPI >= EPI_T64 ? 7 : 8);
+}
 
 // Polarised exit terms of a finished ray (SBR_POL_HHVV): the HH and VV amplitudes
 // and the physical exit path L + (plane - s.p_last), i.e. the path from the launch
@@ -147,7 +152,7 @@ __device__ __forceinline__ void add_fixed(unsigned long long* acc, double v, dou
 // point, to one of the segment's accumulator replicas.  Which lane takes which
 // ray depends only on the item, so every sum is reproducible bit for bit.
 template <int PREC, int EPI, bool REC, bool POL, bool MULTI, bool W8 = false>
-__global__ void __launch_bounds__(kCtaThreads, kMinCtasPerSm) k_trace(const TraceParams P) {
+__global__ void __launch_bounds__(kCtaThreads, min_ctas_per_sm<EPI>()) k_trace(const TraceParams P) {
     constexpr unsigned FULL = 0xffffffffu;
     constexpr bool F64 = PREC == SBR_PREC_FP64;
     constexpr bool TRANSPOSED = Epi<EPI>::kTransposed;
