@@ -99,9 +99,10 @@ __device__ __forceinline__ void start_f(RayF& r, const Segment& G, const JobCons
 // One closest-hit query, then reflect and nudge; true when the ray is finished.
 // The first query is read from the first-hit buffer when there is one (and the
 // entry is restored to empty for the next chunk).
-template <int PREC, bool REC, bool POL, bool W8 = false>
+// SPEC: the speculative closest-hit walk, entered by all lanes of `mask` together.
+template <int PREC, bool REC, bool POL, bool W8 = false, bool SPEC = false>
 __device__ __forceinline__ bool step_f(RayF& r, PolF& e, const SceneView& S, int maxB, uint32_t& err,
-                                       sbr_ray_record* rec, unsigned long long* zbuf) {
+                                       sbr_ray_record* rec, unsigned long long* zbuf, unsigned mask = 0u) {
     float tB = 1e20f;
     int slot;
     if (zbuf != nullptr && r.count == 0) {
@@ -110,6 +111,9 @@ __device__ __forceinline__ bool step_f(RayF& r, PolF& e, const SceneView& S, int
         if (key == ~0ull) return true;
         tB = __uint_as_float((unsigned)(key >> 32));
         slot = (int)(unsigned)key;
+    } else if constexpr (SPEC) {
+        static_assert(PREC == SBR_PREC_MIXED && !REC && !POL && !W8, "the speculative walk is the mixed scalar sweep's");
+        slot = closest_speculative(S, r.o, r.d, 1.0e-3f, tB, err, mask);
     } else if constexpr (W8) {
         static_assert(PREC == SBR_PREC_MIXED && !REC && !POL, "the 8-wide walk is the mixed scalar sweep's");
         slot = Walker8::closest(S, r.o, r.d, 1.0e-3f, tB, err);

@@ -72,6 +72,11 @@ inline int pick_epi(int channels) {
 // layouts, trihedral (1 channel) 50,993 / 49,455 / 47,565 samples/s at 8 / 7 / 6
 // CTAs (64 / 72 / 80 registers); lane-owned layouts, aircraft (64 channels)
 // 13,180 / 13,499 / 12,948.  SBR_TRACE_CTAS_PER_SM (build flag) overrides both.
+// SBR_TRACE_SPECULATIVE=1 (build flag): the mixed scalar sweep walks with the
+// speculative closest-hit walk (trace.cuh) instead of the per-lane while-while one.
+#ifndef SBR_TRACE_SPECULATIVE
+#define SBR_TRACE_SPECULATIVE 0
+#endif
 #ifndef SBR_TRACE_CTAS_PER_SM
 #define SBR_TRACE_CTAS_PER_SM 0
 #endif
@@ -250,9 +255,19 @@ __global__ void __launch_bounds__(kCtaThreads, min_ctas_per_sm<EPI>()) k_trace(c
             bool done = false;
             RayOut out;
             out.amp = 0.0f;
+            // the speculative walk is entered by the active lanes together (first hits
+            // from the raster buffer skip the walk, so it is not used with one)
+            constexpr bool SPEC = SBR_TRACE_SPECULATIVE && PREC == SBR_PREC_MIXED && !REC && !POL && !W8;
+            const unsigned amask = SPEC ? __ballot_sync(FULL, active) : 0u;
             if (active) {
-                done = F64 ? step_d<REC, POL>(rd, ed, S, J.max_bounces, err, rec)
-                           : step_f<PREC, REC, POL, W8>(rf, ef, S, J.max_bounces, err, rec, P.zbuf);
+                if constexpr (SPEC) {
+                    done = P.zbuf == nullptr
+                               ? step_f<PREC, REC, POL, W8, true>(rf, ef, S, J.max_bounces, err, rec, nullptr, amask)
+                               : step_f<PREC, REC, POL, W8>(rf, ef, S, J.max_bounces, err, rec, P.zbuf);
+                } else {
+                    done = F64 ? step_d<REC, POL>(rd, ed, S, J.max_bounces, err, rec)
+                               : step_f<PREC, REC, POL, W8>(rf, ef, S, J.max_bounces, err, rec, P.zbuf);
+                }
                 ++queries;
                 if (done) {
                     const int cnt = F64 ? rd.count : rf.count;

@@ -563,6 +563,126 @@ struct Walker8 {
     }
 };
 
+// Speculative variant of Walker<false>::closest with the watertight test (Aila and
+// Laine, "Understanding the Efficiency of Ray Traversal on GPUs", HPG 2009): a lane
+// that reaches a leaf parks it and keeps walking inner nodes (pruning with its not
+// yet lowered closest distance) until every lane of `mask` holds a parked leaf or
+// has emptied its stack; then all lanes test their leaves.  Every lane of `mask`
+// calls it together and leaves it together (each runs the same sequence of
+// __any_sync); a lane whose iteration budget runs out stops walking but stays in
+// step, and returns -1 with DEV_ERR_BUDGET.
+__device__ __forceinline__ int closest_speculative(const SceneView& S, F3 o, F3 d, float tMin, float& tBest,
+                                                   uint32_t& err, unsigned mask) {
+    const F3 inv{slab_inv(d.x), slab_inv(d.y), slab_inv(d.z)};
+    const WtRay wr = wt_ray(d);
+    const F3 oi{o.x * inv.x, o.y * inv.y, o.z * inv.z};
+    const Slab2 R2 = slab2(inv, oi);
+    const unsigned onx = inv.x < 0.0f ? 16u : 0u, ony = inv.y < 0.0f ? 48u : 32u, onz = inv.z < 0.0f ? 80u : 64u;
+    const unsigned ofx = onx ^ 16u, ofy = ony ^ 16u, ofz = onz ^ 16u;
+    unsigned long long stack[kStackDepth];
+    int sp = 0;
+    int ref = 0;        // current entry: inner node (>= 0) or leaf (< 0), valid while `has`
+    bool has = true;
+    int parked = 0;     // a leaf waiting to be tested (< 0), or 0
+    int best = -1;
+    bool over = false;
+    uint32_t iters = 0;
+    auto plane = [](const GNode4* p, unsigned off) {
+        return __ldg(reinterpret_cast<const float4*>(reinterpret_cast<const char*>(p) + off));
+    };
+    auto push = [&](int r, float t) {
+        if (sp < kStackDepth) stack[sp++] = pack_entry(r, t);
+        else err |= DEV_ERR_STACK;
+    };
+    auto pop = [&]() {
+        while (sp > 0) {
+            const unsigned long long e = stack[--sp];
+            if (__uint_as_float((unsigned)(e >> 32)) <= tBest) { ref = (int)(unsigned)e; return true; }
+        }
+        return false;
+    };
+    auto test_leaf = [&](int leaf) {
+        const int code = ~leaf;
+        const int first = code >> 4, cnt = code & 15;
+        switch (wr.kz) {
+            case 0: leaf_wt<0>(S.tris, first, cnt, o, wr, tMin, tBest, best); break;
+            case 1: leaf_wt<1>(S.tris, first, cnt, o, wr, tMin, tBest, best); break;
+            default: leaf_wt<2>(S.tris, first, cnt, o, wr, tMin, tBest, best); break;
+        }
+    };
+    for (;;) {
+        // inner nodes, while some lane holds an entry but no parked leaf
+        while (__any_sync(mask, has && parked == 0)) {
+            if (has && ref >= 0) {
+                if (++iters > kIterBudget) {
+                    over = true;
+                    has = false;
+                    parked = 0;
+                } else {
+                    const GNode4* np = S.nodes + ref;
+                    const float4 nx = plane(np, onx), fx = plane(np, ofx), ny = plane(np, ony), fy = plane(np, ofy);
+                    const float4 nz = plane(np, onz), fz = plane(np, ofz);
+                    const int4 ch = __ldg(&np->child);
+                    float t[4];
+                    bool hh[4];
+                    slab4_nh(nx, fx, ny, fy, nz, fz, R2, tMin, tBest, t, hh);
+                    const bool h0 = hh[0], h1 = hh[1], h2 = hh[2], h3 = hh[3];
+                    int c[4] = {ch.x, ch.y, ch.z, ch.w};
+                    const int nh = int(h0) + int(h1) + int(h2) + int(h3);
+                    if (nh == 1) {
+                        ref = h0 ? c[0] : h1 ? c[1] : h2 ? c[2] : c[3];
+                    } else if (nh == 2) {
+                        const float ta = h0 ? t[0] : h1 ? t[1] : t[2];
+                        const int ca = h0 ? c[0] : h1 ? c[1] : c[2];
+                        const float tb = h3 ? t[3] : h2 ? t[2] : t[1];
+                        const int cb = h3 ? c[3] : h2 ? c[2] : c[1];
+                        const bool sw = tb < ta;
+                        push(sw ? ca : cb, sw ? ta : tb);
+                        ref = sw ? cb : ca;
+                    } else if (nh > 2) {
+                        const float inf = __int_as_float(0x7f800000);
+                        t[0] = h0 ? t[0] : inf;
+                        t[1] = h1 ? t[1] : inf;
+                        t[2] = h2 ? t[2] : inf;
+                        t[3] = h3 ? t[3] : inf;
+                        sort4(t, c);
+                        if (t[3] <= tBest) push(c[3], t[3]);
+                        if (t[2] <= tBest) push(c[2], t[2]);
+                        push(c[1], t[1]);
+                        ref = c[0];
+                    } else {
+                        has = pop();
+                    }
+                }
+            }
+            if (has && ref < 0 && parked == 0) {  // a leaf: park it and walk on
+                parked = ref;
+                has = pop();
+            }
+        }
+        // leaves: the parked one, then this lane's run of leaf entries
+        if (parked != 0) {
+            test_leaf(parked);
+            parked = 0;
+        }
+        while (has && ref < 0) {
+            if (++iters > kIterBudget) {
+                over = true;
+                has = false;
+                break;
+            }
+            test_leaf(ref);
+            has = pop();
+        }
+        if (!__any_sync(mask, has)) break;
+    }
+    if (over) {
+        err |= DEV_ERR_BUDGET;
+        return -1;
+    }
+    return best;
+}
+
 template <>
 struct Walker<true> {
     __device__ __forceinline__ static int closest(const SceneView& S, D3 o, D3 d, double tMin, double& tBest,
