@@ -488,7 +488,7 @@ def run_uneven(args, torch, sbr, dist, ws, rank, local):
     line = {
         "metric": "angle-freq samples/s", "value": samples / (step_ms * 1e-3), "unit": "samples/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
-        "scaling": "strong", "vs_baseline": None, "dtype": "fp32 traversal + fp64 phase/sums",
+        "scaling": "strong", "vs_baseline": None, "dtype": "fp32 traversal + fp32-pair phase + fp64 sums",
         "data": "synthetic (seeded uneven batch of 64 meshes)",
         "config": {"workload": f"uneven_64meshes_{min(tri)}-{max(tri)}tri_{int(sum(len(b['phi']) for b in batch))}samples",
                    "meshes": len(batch), "triangles_total": int(sum(tri)), "samples": int(samples),
@@ -812,7 +812,7 @@ def main():
     line = {
         "metric": "angle-freq samples/s", "value": value, "unit": "samples/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
-        "scaling": "strong" if ws > 1 else "weak", "vs_baseline": None, "dtype": "fp32 traversal + fp64 phase/sums",
+        "scaling": "strong" if ws > 1 else "weak", "vs_baseline": None, "dtype": "fp32 traversal + fp32-pair phase + fp64 sums",
         "data": f"synthetic (seeded {args.workload} mesh)",
         "config": config_of(w),
         "run": {"rays_launched_per_step": info["n_rays_clipped"], "mode": "batched persistent",

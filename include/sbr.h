@@ -127,7 +127,7 @@ typedef struct sbr_job {
                                  frequencies of a job come from one trace */
 #define SBR_MODE_PER_ANGLE 1  /* the reference's loop: one trace + PO launch per (angle, frequency) */
 
-#define SBR_PREC_MIXED 0      /* FP32 traversal, FP64 path length / phase reduction / field sums */
+#define SBR_PREC_MIXED 0      /* FP32 traversal, FP64 path length, FP32-pair phase reduction, FP64 field sums */
 #define SBR_PREC_FP32 1       /* the reference FP32 build's arithmetic (launch plane at 10 G, FP32 phase) */
 #define SBR_PREC_FP64 2       /* everything in FP64 (the reference USE_DOUBLE build's arithmetic) */
 
@@ -241,8 +241,9 @@ sbr_status sbr_run(sbr_scene* scene, const sbr_job* jobs, size_t n_jobs, sbr_res
  * rays differ by rounding only: the part of those errors that is the same for all
  * rays seeing the same geometry the same way (the systematic rounding of the hit
  * distance, the sine / cosine approximation) is bounded coherently, as a fraction
- * of |field|, the rest (independent from ray to ray) by a probabilistic
- * rounding-error bound exceeded with probability below 6e-8.
+ * of |field|, the rest (independent from ray to ray, and the FP32 partial sums of
+ * each 4x8 ray block) by a probabilistic rounding-error bound exceeded with
+ * probability below 6e-8.
  *   field     [n_samples * 2] in: the mixed-precision fields sbr_run returned.
  *   err_field [n_samples] out (may be NULL): stated |field - field_FP64|.
  *   err_db    [n_samples] out (may be NULL): the |dBsm - dBsm_FP64| it implies (dBsm

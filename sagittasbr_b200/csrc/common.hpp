@@ -153,6 +153,7 @@ struct FreqConst {
     double turns;         // k / pi
     float kf;
     float scalef;
+    float turns_hi, turns_lo;  // k / pi as an unevaluated FP32 pair (hi + lo)
 };
 
 struct ItemStats {

@@ -1,6 +1,6 @@
 // errbound.cu -- sbr_error_bound: the error, per (angle, frequency) sample, of the
-// mixed-precision sweep (FP32 traversal, FP64 path and sums) against the FP64
-// sweep of the same job.  No counterpart in the reference, which has no
+// mixed-precision sweep (FP32 traversal, FP64 path, FP32 phase pairs, FP64 sums of
+// FP32 block partials) against the FP64 sweep of the same job.  No counterpart in the reference, which has no
 // mixed-precision mode.
 //
 // A second pass re-traces every ray of the plan with the mixed sweep's own
@@ -35,8 +35,15 @@
 // sample
 //   E_k = |Delta_k| + |S_k| (2 k c1 + eps) + lambda scale_k (2 k sqrt(Q1) + sqrt(Q0))
 //         + (items + 1) quantum_k,
+//         + lambda scale_k u sqrt(Q2),
 // Q1 = sum (amp (dL - dLs))^2, Q0 = sum damp^2 over the rounding-only rays; the
-// last term covers the fixed-point fold of the sweep.
+// fixed-point term covers the fixed-point fold of the sweep.  The last term covers
+// the FP32 partial sums of the lane-owned epilogue: each term of a 4x8 ray block is
+// added to its channel's FP32 partial by one FMA, rounded within u |partial|, and
+// every partial is within A_b = sum |amp| of the block, so Q2 = sum over blocks of
+// n_b A_b^2 (n_b terms); the per-lane layouts sum in FP64 and the term only
+// overstates their error.  The phase pair's 2^-45 |x| turns (ray.cuh, turns_frac)
+// is added to dLs as 2^-45 L.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -48,8 +55,9 @@ namespace sbr {
 namespace {
 
 constexpr float kU = 5.9604644775390625e-08f;  // 2^-24, unit roundoff of FP32
-// Phase / amplitude error of one mixed term: the FP32 remainder of 2 k L in turns
-// (2 pi 2^-25 rad), __sincosf (below 4e-7 absolute), FP32 amplitude (2^-24).
+// Phase / amplitude error of one mixed term: the rounding of the FP32 remainder of
+// 2 k L in turns (2 pi 2^-25 rad; the FP32 pair's 2^-45 |x| is carried in dLs),
+// __sincosf (below 4e-7 absolute), FP32 amplitude (2^-24).
 constexpr double kPhaseEps = 1.0e-6;
 
 constexpr double kPhaseExact = 0.05;  // rad: rays with more phase uncertainty are re-traced in FP64
@@ -64,7 +72,7 @@ struct ErrParams {
     const FreqConst* freqs;
     int64_t n_items;
     unsigned long long* queue;
-    double* acc;       // [n_segs][8]: sum amp, sum amp dLs, -, Q1, Q0, re-traced rays, rays, -
+    double* acc;       // [n_segs][8]: sum amp, sum amp dLs, Q2, Q1, Q0, re-traced rays, rays, -
     double* dfield;    // [n_samples][2]: sum of (FP64 term - mixed term) of the re-traced rays
     float diag;        // scene bounding-box diagonal (m)
     uint32_t* err;
@@ -214,7 +222,8 @@ __device__ int closest_flag(const SceneView& S, F3 o, F3 d, float tMin, float& t
 // with the uncertainty bounds carried along; rays near a decision or with a large
 // phase uncertainty are re-traced with the FP64 sweep's own step and their term
 // differences added to dfield, the others add to the lane's sums of squares.
-__device__ __forceinline__ void ray_bound(const ErrParams& P, const Segment& G, const JobConst& J, const FreqConst* F,
+// Returns the amplitude the sweep adds for the ray (0 when it adds nothing).
+__device__ __forceinline__ float ray_bound(const ErrParams& P, const Segment& G, const JobConst& J, const FreqConst* F,
                                          int K, double kmax, int i, int j, double& sa, double& s1, double& q1,
                                          double& s0, unsigned& nex, uint32_t& err) {
     RayF r;
@@ -262,6 +271,8 @@ __device__ __forceinline__ void ray_bound(const ErrParams& P, const Segment& G, 
         dnl = dnrm;
     }
     const RayOut om = finish_f<SBR_PREC_MIXED>(r, J);
+    dLs += ldexp(om.L, -45);  // the FP32 phase pair (ray.cuh, turns_frac)
+    dL += ldexp(om.L, -45);
     if (amb || (r.count > 0 && 2.0 * kmax * dL > kPhaseExact)) {
         // the FP64 sweep's own ray (start_d / step_d) and the exact term differences
         RayD rd;
@@ -291,6 +302,7 @@ __device__ __forceinline__ void ray_bound(const ErrParams& P, const Segment& G, 
         q1 += e1 * e1;
         s0 += e0 * e0;
     }
+    return om.amp;
 }
 
 __global__ void __launch_bounds__(kCtaThreads) k_errbound(const ErrParams P) {
@@ -316,21 +328,29 @@ __global__ void __launch_bounds__(kCtaThreads) k_errbound(const ErrParams P) {
         for (int k = 0; k < J.n_freqs; ++k) kmax = fmax(kmax, F[k].k);
         const int b0 = int(item - G.item_base) * G.blocks_per_item;
         const int b1 = min(b0 + G.blocks_per_item, G.blocks);
-        double sa = 0.0, s1 = 0.0, q1 = 0.0, s0 = 0.0;
+        double sa = 0.0, s1 = 0.0, q1 = 0.0, s0 = 0.0, q2 = 0.0;
         unsigned nex = 0, nray = 0;
         for (int blk = b0; blk < b1; ++blk) {
             const int i = G.i0 + (blk % G.blocks_x) * kBlockW + (lane % kBlockW);
             const int j = G.j0 + (blk / G.blocks_x) * kBlockH + (lane / kBlockW);
+            float am = 0.0f;
             if (i < G.i0 + G.ni && j < G.j0 + G.nj) {
-                ray_bound(P, G, J, F, J.n_freqs, kmax, i, j, sa, s1, q1, s0, nex, err);
+                am = ray_bound(P, G, J, F, J.n_freqs, kmax, i, j, sa, s1, q1, s0, nex, err);
                 ++nray;
             }
+            // the block's FP32 partial sums: n_b terms, every partial within A_b
+            double ab = double(fabsf(am));
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) ab += __shfl_xor_sync(FULL, ab, off);
+            const int nb = __popc(__ballot_sync(FULL, am != 0.0f));
+            if (lane == 0) q2 += double(nb) * ab * ab;
         }
         for (int off = 16; off > 0; off >>= 1) {
             sa += __shfl_xor_sync(FULL, sa, off);
             s1 += __shfl_xor_sync(FULL, s1, off);
             q1 += __shfl_xor_sync(FULL, q1, off);
             s0 += __shfl_xor_sync(FULL, s0, off);
+            q2 += __shfl_xor_sync(FULL, q2, off);
         }
         nex = __reduce_add_sync(FULL, nex);
         nray = __reduce_add_sync(FULL, nray);
@@ -338,6 +358,7 @@ __global__ void __launch_bounds__(kCtaThreads) k_errbound(const ErrParams P) {
             double* A = P.acc + 8 * seg;
             atomicAdd(A, sa);
             atomicAdd(A + 1, s1);
+            atomicAdd(A + 2, q2);
             atomicAdd(A + 3, q1);  // sums of squares of independent per-ray bounds
             atomicAdd(A + 4, s0);
             atomicAdd(A + 5, double(nex));
@@ -443,7 +464,7 @@ extern "C" sbr_status sbr_error_bound(sbr_scene* s, const sbr_job* jobs, size_t 
                 const double shared = a * ((A[0] > 0.0 ? 2.0 * F.k * A[1] / A[0] : 0.0) + kPhaseEps);
                 const double E = std::hypot(dfield[2 * smp], dfield[2 * smp + 1]) + shared +
                                  kLambda * F.scale * (2.0 * F.k * std::sqrt(A[3]) + std::sqrt(A[4])) +
-                                 double(items + 1) * F.quantum;
+                                 double(items + 1) * F.quantum + kLambda * F.scale * double(kU) * std::sqrt(A[2]);
                 if (err_field) err_field[smp] = E;
                 if (err_db) {
                     const double db = 10.0 * std::log10(std::max(4.0 * M_PI * a * a, 1e-10));

@@ -187,6 +187,8 @@ sbr_status build_tables(const sbr_scene* const* scenes, const int32_t* job_scene
             fc.k = 2.0 * M_PI / lambda;
             fc.scale = fc.k * area / (4.0 * M_PI);
             fc.turns = fc.k / M_PI;
+            fc.turns_hi = float(fc.turns);
+            fc.turns_lo = float(fc.turns - double(fc.turns_hi));
             float lambdaf = 299792458.0f / float(J.freq_hz[f]);
             fc.kf = 2.0f * float(M_PI) / lambdaf;
             fc.scalef = fc.kf * areaf / (4.0f * float(M_PI));

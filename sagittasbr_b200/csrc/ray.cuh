@@ -34,6 +34,7 @@ struct RayOut {
     double cosD, RnD;
     double pa[2];  // SBR_POL_HHVV: co-polarised amplitudes (HH, VV)
     double Lp;     // SBR_POL_HHVV: path launch plane -> exit point -> launch plane
+    float Lh, Ll;  // MIXED: the phase path (L, or Lp / 2 for SBR_POL_HHVV) as an FP32 pair
 };
 
 // Polarisation state of SBR_POL_HHVV plans: the HH and VV incident fields as they
@@ -63,6 +64,12 @@ __device__ __forceinline__ D3 pec_reflect(D3 e, D3 n) {
 template <class V, class R>
 __device__ __forceinline__ R pol_amp(V e, V n, V d, V E, R twoRn) {
     return twoRn * dot(e, cross(n, cross(d, E)));
+}
+
+// x as an unevaluated FP32 pair hi + lo (|x - hi - lo| <= 2^-48 |x|).
+__device__ __forceinline__ void split_f32(double x, float& hi, float& lo) {
+    hi = float(x);
+    lo = float(x - double(hi));
 }
 
 // ------------------------------------------------------------ FP32 / mixed
@@ -156,6 +163,7 @@ __device__ __forceinline__ RayOut finish_f(const RayF& r, const JobConst& J) {
     o.dist32 = r.dist32;
     o.L = (PREC == SBR_PREC_FP32) ? double(r.dist32) : r.L;
     o.amp = (r.count > 0 && c > 0.0f) ? 2.0f * c * Rn : 0.0f;
+    split_f32(o.L, o.Lh, o.Ll);
     return o;
 }
 
@@ -212,22 +220,35 @@ __device__ __forceinline__ RayOut finish_d(const RayD& r, const JobConst& J) {
     o.L = r.L;
     o.dist32 = float(r.L);
     o.amp = (r.count > 0 && c > 0.0) ? float(2.0 * c * Rn) : 0.0f;
+    split_f32(o.L, o.Lh, o.Ll);
     return o;
 }
 
 // ------------------------------------------------------------ PO term
-// sin and cos of 2 pi x for a phase x given in turns (FP64): the whole turns are
-// removed exactly (x - rint(x) is exact for |x| < 2^52), the remainder in
-// [-1/2, 1/2] is rounded to FP32 (an absolute error below 3e-8 turns) and its
-// sine and cosine are taken in FP32.
-__device__ __forceinline__ void sincos_turns(double x, float& s, float& c) {
-    const float r = float(x - rint(x));
-    __sincosf(6.28318530717958647692f * r, &s, &c);
+// The MIXED phase, (k / pi) L turns, is formed and reduced in FP32 arithmetic on
+// unevaluated pairs (hi + lo; Dekker, Numer. Math. 18, 1971): the product of the
+// leading parts is split exactly into p + e by one FMA, the cross products are
+// added to e, and the whole turns are taken from p alone, p - rint(p) being exact
+// in FP32.  The remainder r = (p - rint(p)) + e lies within 2^-25 + 2^-45 |x|
+// turns of the exact one (x = k L / pi; |x| < 2^17, a 1 km path at 18 GHz, gives
+// 3.4e-8 turns) and |r| <= 1/2 + 2^-24 |x|.  No FP64 operation and no
+// conversion per (ray, frequency): only the sine and cosine use the special
+// function unit.
+__device__ __forceinline__ float turns_frac(float th, float tl, float Lh, float Ll) {
+    const float p = th * Lh;
+    float e = fmaf(th, Lh, -p);
+    e = fmaf(th, Ll, e);
+    e = fmaf(tl, Lh, e);
+    return (p - rintf(p)) + e;
+}
+// sin and cos of the MIXED phase of path (Lh + Ll) at frequency F.
+__device__ __forceinline__ void sincos_mixed(const FreqConst& F, float Lh, float Ll, float& s, float& c) {
+    __sincosf(6.28318530717958647692f * turns_frac(F.turns_hi, F.turns_lo, Lh, Ll), &s, &c);
 }
 
 // PO term of one ray at one frequency, added to (re, im).
 //  FP32: the reference FP32 arithmetic (phase fmodf in FP32).
-//  MIXED: phase 2 k L = 2 pi (k / pi) L reduced in turns (sincos_turns); the
+//  MIXED: phase 2 k L = 2 pi (k / pi) L reduced in turns (sincos_mixed); the
 //         term is summed without the factor k A / (4 pi), which the item fold
 //         applies once per channel.
 //  FP64: the reference USE_DOUBLE arithmetic.
@@ -243,7 +264,7 @@ __device__ __forceinline__ void po_term(int prec, const FreqConst& F, const RayO
         im += double(mag * c);
     } else if (prec == SBR_PREC_MIXED) {
         float s, c;
-        sincos_turns(F.turns * r.L, s, c);
+        sincos_mixed(F, r.Lh, r.Ll, s, c);
         const double a = double(r.amp);
         re -= a * double(s);
         im += a * double(c);

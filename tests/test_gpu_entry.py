@@ -96,7 +96,9 @@ def test_cli_frequency_scan_matches_python_driver_and_mie(tmp_path):
     np.testing.assert_array_equal(cli[:, 0], fr)
     np.testing.assert_allclose(cli[:, 1], mean, rtol=1e-12)
     np.testing.assert_allclose(cli[:, 2], std, rtol=1e-9)
-    np.testing.assert_allclose(mean, one, rtol=1e-9)
+    # the 5-frequency trace sums each 4x8 ray block in FP32 first (lane-owned
+    # epilogue), the 1-frequency traces sum in FP64
+    np.testing.assert_allclose(mean, one, rtol=1e-5)
     mie_sigma = np.array([mie.sphere_rcs(1.0, f) for f in fr])
     assert np.all(np.abs(mean / mie_sigma - 1.0) < 0.15), mean / mie_sigma
 
@@ -110,4 +112,6 @@ def test_frequency_scan_with_more_than_128_frequencies():
         th, ph = sbr.config_angles(cfg)
         ref = sbr.run(sc, sbr.JobSpec(th, ph, fr[128:], 64, 64, 2.2, 2)).sigma_m2.reshape(4, 2).mean(axis=0)
     assert fr.size == 130 and mean.size == 130
-    np.testing.assert_allclose(mean[128:], ref, rtol=1e-9)
+    # the scan's plan holds a 128-frequency job, so its 2-frequency job is summed in
+    # the lane-owned layout (FP32 block partials) and its own run per lane in FP64
+    np.testing.assert_allclose(mean[128:], ref, rtol=1e-5)

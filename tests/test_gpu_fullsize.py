@@ -9,8 +9,10 @@ frequency, 5 bounces.
 * mixed precision against the reference's own USE_DOUBLE GPU build (baseline/_ref)
   on two azimuths, same bar;
 * the batched trace equals per-frequency traces on the same grid (one trace serves
-  all frequencies) to 1e-12 of the largest field; the per-item FP64 partial sums
-  are ordered differently by the two epilogue layouts, so not bit for bit.
+  all frequencies): the lane-owned epilogue of the 8-frequency trace sums each 4x8
+  ray block in FP32 before the FP64 sums, the per-lane one of a 1-frequency trace
+  sums in FP64, so they agree within the stated error and to 1e-5 of the largest
+  field, not bit for bit.
 """
 import numpy as np
 import pytest
@@ -63,9 +65,14 @@ def test_mixed_unfiltered_within_stated_error(aircraft):
 
 def test_one_trace_equals_per_frequency_traces(aircraft):
     f = aircraft["mixed"].field.reshape(len(AZ), len(FREQS))
+    e = aircraft["err_field"].reshape(len(AZ), len(FREQS))
     for r, k in zip(aircraft["per_f"], range(0, len(FREQS), 3)):
         g = r.field.reshape(len(AZ))
-        assert np.abs(g - f[:, k]).max() <= 1e-12 * np.abs(f[:, k]).max()
+        d = np.abs(g - f[:, k])
+        print(f"{FREQS[k] / 1e9:.2f} GHz: one trace vs per-frequency trace, max |d field| / max |field| "
+              f"{d.max() / np.abs(f[:, k]).max():.2e}")
+        assert np.all(d <= e[:, k])
+        assert d.max() <= 1e-5 * np.abs(f[:, k]).max()
 
 
 def test_mixed_within_0p1_db_of_reference_double_build(aircraft):

@@ -1,6 +1,9 @@
 """GPU checks of multi-scene plans (sbr_plan_create_multi): jobs over different
-meshes in one persistent launch give, bit for bit, the fields of separate
-single-scene runs (the fixed-point sums do not depend on which warp adds what)."""
+meshes in one persistent launch give the fields of separate single-scene runs (the
+fixed-point sums do not depend on which warp adds what): to 1e-12 when the plan's
+accumulator layout is each job's own, and within the FP32 partial sums of the
+mixed lane-owned layout (below 1e-5) when the plan's widest job selects it for
+jobs whose own runs sum per lane in FP64."""
 import numpy as np
 import pytest
 
@@ -43,8 +46,12 @@ def test_multi_scene_plan_matches_separate_runs(prec, pol, mode):
         want = [sbr.run(scenes[s], j, mode=mode, precision=prec, polarization=pol) for j, s in zip(jobs, job_scene)]
         want_f = np.concatenate([w.field for w in want])
         # the same sums, up to the order of FP64 additions inside a warp when the plan's
-        # widest job selects another accumulator layout than a job's own run
-        np.testing.assert_allclose(got.field, want_f, rtol=1e-12, atol=1e-13 * np.abs(want_f).max())
+        # widest job selects another accumulator layout than a job's own run; the
+        # mixed lane-owned layout (more than 4 channels: the HH + VV plan) also sums
+        # each 4x8 ray block in FP32 first
+        wide = prec == sbr.PREC_MIXED and pol == sbr.POL_HHVV
+        rtol, atol = (1e-5, 1e-6) if wide else (1e-12, 1e-13)
+        np.testing.assert_allclose(got.field, want_f, rtol=rtol, atol=atol * np.abs(want_f).max())
         assert np.array_equal(got.stats, np.concatenate([w.stats for w in want]))
     finally:
         for s in scenes:

@@ -8,7 +8,7 @@ as ambiguous (a decision within 1e-6 m / 1e-6 relative of flipping: shared
 edges, |det| at the 1e-6 threshold, ties in t, t at tMin), each of which can
 change the sum by at most 2 * max|term|, and amp_r = 2 cos(theta) R^n is the
 magnitude of ray r's term.  eps is the per-ray phase/amplitude error of the
-precision mode: 1e-9 (FP64), 1e-4 (mixed: FP32 traversal, FP64 phase), 3e-3
+precision mode: 1e-9 (FP64), 1e-4 (mixed: FP32 traversal, FP32-pair phase), 3e-3
 (FP32: the reference FP32 build's arithmetic, FP32 phase at 10 G).
 Hit sequences must be identical for every ray the oracle does not flag.
 """
