@@ -624,8 +624,10 @@ def main():
     ap.add_argument("--no-per-angle", action="store_true", help="skip the per-angle mode measurement")
     ap.add_argument("--per-angle-stride", type=int, default=8,
                     help="per-angle mode is timed on every n-th angle of the sweep")
-    ap.add_argument("--first-hit", default="traverse", choices=["traverse", "raster"],
-                    help="first closest hit by BVH walk (default) or by the first-hit raster")
+    ap.add_argument("--first-hit", default="auto", choices=["auto", "traverse", "raster"],
+                    help="first closest hit: the library's choice (default: the tile raster where a plan launches "
+                         ">= 8 rays per triangle per angle), the BVH walk, or the tile raster")
+    ap.add_argument("--tile-cap", type=int, default=0, help="the raster's per-tile triangle list length (0: 48)")
     ap.add_argument("--autotune", action="store_true",
                     help="let the plan time candidate work-item sizes / grid sizes on a sample first")
     ap.add_argument("--polarization", default="scalar", choices=["scalar", "hhvv"],
@@ -673,15 +675,18 @@ def main():
     scene_s = time.perf_counter() - t_scene
     sah_ms = scene.info()["sah_ms"]
     job = sbr.JobSpec(w["theta"], w["phi"], w["freqs"], w["nx"], w["ny"], w["G"], w["max_bounces"], w["R"])
-    first_hit = sbr.FIRST_HIT_RASTER if args.first_hit == "raster" else sbr.FIRST_HIT_TRAVERSE
+    first_hit = {"auto": sbr.FIRST_HIT_AUTO, "raster": sbr.FIRST_HIT_RASTER,
+                 "traverse": sbr.FIRST_HIT_TRAVERSE}[args.first_hit]
     pol = sbr.POL_HHVV if args.polarization == "hhvv" else sbr.POL_SCALAR
     from sagittasbr_b200.sharding import ShardedPlan
     t_plan = time.perf_counter()
     shard = ShardedPlan(scene, job, rank, ws, mode=sbr.MODE_BATCHED, precision=sbr.PREC_MIXED, stream=sp,
-                        first_hit=first_hit, polarization=pol, autotune=args.autotune) if ws > 1 else None
+                        first_hit=first_hit, polarization=pol, autotune=args.autotune,
+                        tile_cap=args.tile_cap) if ws > 1 else None
     plan = shard.plan if shard is not None else sbr.Plan(scene, [job], mode=sbr.MODE_BATCHED,
                                                          precision=sbr.PREC_MIXED, stream=sp, first_hit=first_hit,
-                                                         polarization=pol, autotune=args.autotune)
+                                                         polarization=pol, autotune=args.autotune,
+                                                         tile_cap=args.tile_cap)
     plan_s = time.perf_counter() - t_plan
     info = plan.info if plan is not None else {"n_samples": 0, "n_rays_clipped": 0, "launches_per_execute": 0,
                                                "blocks_per_item": 0, "ctas_per_sm": 0, "h2d_bytes": 0,
@@ -743,10 +748,10 @@ def main():
         t0 = time.perf_counter()
         if shard is None:
             r2 = sbr.run(scene, job, mode=sbr.MODE_BATCHED, precision=sbr.PREC_MIXED, first_hit=first_hit,
-                         polarization=pol, blocks_per_item=info["blocks_per_item"])
+                         polarization=pol, blocks_per_item=info["blocks_per_item"], tile_cap=args.tile_cap)
         else:
             e2 = ShardedPlan(scene, job, rank, ws, mode=sbr.MODE_BATCHED, precision=sbr.PREC_MIXED, stream=sp,
-                             first_hit=first_hit, polarization=pol)
+                             first_hit=first_hit, polarization=pol, tile_cap=args.tile_cap)
             e2.execute()
             r2 = e2.gather(torch)
             e2.close()
@@ -821,7 +826,9 @@ def main():
                                 "inside the timed region") if ws > 1 else "1 GPU",
                 "scene_build_s": scene_s, "sah_build": {"where": "gpu" if args.gpu_build else "host", "ms": sah_ms},
                 "plan_s": plan_s, "autotune": bool(args.autotune), "node_width": args.node_width,
-                "blocks_per_item": info["blocks_per_item"], "ctas_per_sm": info["ctas_per_sm"]},
+                "blocks_per_item": info["blocks_per_item"], "ctas_per_sm": info["ctas_per_sm"],
+                "first_hit": {sbr.FIRST_HIT_RASTER: "tile raster", sbr.FIRST_HIT_TRAVERSE: "walk"}.get(
+                    info.get("first_hit"), None), "tile_cap": args.tile_cap or 48},
         "mray_bounces_per_s": bounces_all / (step_ms * 1e-3) / 1e6,
         "closest_hit_queries_per_s": queries_all / (step_ms * 1e-3),
         "kernel_ms": kern_ms,

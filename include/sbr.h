@@ -25,7 +25,9 @@
 extern "C" {
 #endif
 
-#define SBR_ABI_VERSION 2  /* 2: sbr_config.error_bound, sbr_build_opts / sbr_run_opts / sbr_plan_info.node_width */
+#define SBR_ABI_VERSION 3  /* 2: sbr_config.error_bound, sbr_build_opts / sbr_run_opts / sbr_plan_info.node_width;
+                              3: SBR_FIRST_HIT_AUTO (0, the default), sbr_run_opts.tile_cap,
+                                 sbr_plan_info.first_hit */
 
 /* ------------------------------------------------------------------ status */
 typedef int32_t sbr_status;
@@ -139,8 +141,11 @@ typedef struct sbr_job {
  * mixed runs (per-angle and FP64 runs always walk).  Measured on B200 it costs
  * about as much as the walk it replaces for coherent ray tubes, so the default
  * walks. */
-#define SBR_FIRST_HIT_TRAVERSE 0  /* walk the BVH for every query (default) */
-#define SBR_FIRST_HIT_RASTER 1    /* first hits from the orthographic first-hit raster */
+#define SBR_FIRST_HIT_AUTO 0      /* (default) the raster where a plan launches, per angle, at least
+                                     8 rays per triangle of its scene; the walk otherwise */
+#define SBR_FIRST_HIT_RASTER 1    /* first hits from the tile-binned orthographic raster (batched
+                                     mixed-precision single-scene plans; others walk) */
+#define SBR_FIRST_HIT_TRAVERSE 2  /* walk the BVH for every query */
 
 /* Polarisation.  SCALAR is the reference's PO term (poKernels.cu:81-109; HH == VV).
  * HHVV (no counterpart in the reference; SBR_PREC_MIXED or SBR_PREC_FP64, at most
@@ -171,7 +176,9 @@ typedef struct sbr_run_opts {
                                  (batched mode; adds about 20 short launches to plan creation) */
     int32_t node_width;       /* tree the mixed-precision scalar sweep walks: 0 -> the scene's widest
                                  (8 when built with sbr_build_opts.node_width = 8), 4, or 8 */
-    int32_t reserved[3];
+    int32_t tile_cap;         /* SBR_FIRST_HIT_RASTER: longest triangle list a 4 x 8 ray tile tests
+                                 (the rays of longer tiles walk the tree); 0 -> 48, at most 1024 */
+    int32_t reserved[2];
 } sbr_run_opts;
 
 /* Results for every (job, angle, frequency[, polarization]) in job order, then
@@ -202,6 +209,7 @@ typedef struct sbr_plan_info {
     int32_t blocks_per_item;  /* the plan's setting (0: automatic per angle) */
     int32_t ctas_per_sm;      /* persistent CTAs per SM of the trace launches */
     int32_t node_width;       /* tree width the plan's mixed scalar sweep walks (4 or 8) */
+    int32_t first_hit;        /* how the plan finds first hits: SBR_FIRST_HIT_RASTER or _TRAVERSE */
 } sbr_plan_info;
 
 sbr_status sbr_plan_create(sbr_scene* scene, const sbr_job* jobs, size_t n_jobs, const sbr_run_opts* opts,

@@ -23,13 +23,13 @@ from typing import Sequence
 import numpy as np
 
 from . import _lib
-from ._lib import (FIRST_HIT_RASTER, FIRST_HIT_TRAVERSE, MODE_BATCHED, MODE_PER_ANGLE, POL_HHVV, POL_SCALAR,
+from ._lib import (FIRST_HIT_AUTO, FIRST_HIT_RASTER, FIRST_HIT_TRAVERSE, MODE_BATCHED, MODE_PER_ANGLE, POL_HHVV, POL_SCALAR,
                    PREC_FP32, PREC_FP64, PREC_MIXED, SbrError, check, lib)
 
 __all__ = [
     "Scene", "JobSpec", "SweepResult", "Plan", "run", "adjoint", "trace_records", "load_config", "config_angles",
     "load_obj", "load_gltf", "load_model", "write_csv", "run_sweep", "freq_scan", "SbrError", "MODE_BATCHED", "MODE_PER_ANGLE", "PREC_MIXED",
-    "FIRST_HIT_RASTER", "FIRST_HIT_TRAVERSE",
+    "FIRST_HIT_AUTO", "FIRST_HIT_RASTER", "FIRST_HIT_TRAVERSE",
     "PREC_FP32", "PREC_FP64", "POL_SCALAR", "POL_HHVV", "RAY_RECORD",
 ]
 
@@ -163,7 +163,7 @@ class SweepResult:
 
 
 def _opts(mode, precision, polarization=POL_SCALAR, stream=None, use_graph=False, ctas_per_sm=0,
-          first_hit=FIRST_HIT_TRAVERSE, blocks_per_item=0, autotune=False, node_width=0):
+          first_hit=FIRST_HIT_AUTO, blocks_per_item=0, autotune=False, node_width=0, tile_cap=0):
     o = _lib.RunOpts()
     o.mode, o.precision, o.polarization = int(mode), int(precision), int(polarization)
     o.use_graph = 1 if use_graph else 0
@@ -173,6 +173,7 @@ def _opts(mode, precision, polarization=POL_SCALAR, stream=None, use_graph=False
     o.blocks_per_item = int(blocks_per_item)
     o.autotune = 1 if autotune else 0
     o.node_width = int(node_width)
+    o.tile_cap = int(tile_cap)
     return o
 
 
@@ -189,16 +190,17 @@ class Plan:
     def __init__(self, scene: Scene | Sequence[Scene], jobs: Sequence[JobSpec], mode=MODE_BATCHED,
                  precision=PREC_MIXED, stream=None, use_graph=False, ctas_per_sm=0, first_hit=None,
                  polarization=POL_SCALAR, job_scene: Sequence[int] | None = None, blocks_per_item=0,
-                 autotune=False, node_width=0):
+                 autotune=False, node_width=0, tile_cap=0):
         """With a list of scenes, job j traces scene[job_scene[j]] (sbr_plan_create_multi).
         autotune=True times candidate (blocks_per_item, ctas_per_sm) settings on a sample of
-        the angles first and keeps the fastest (batched mode); info reports the choice."""
+        the angles first and keeps the fastest (batched mode); info reports the choice.
+        tile_cap: FIRST_HIT_RASTER's longest per-tile triangle list (0: 48, at most 1024)."""
         self.scene = scene
         self.jobs = list(jobs)
         self._jc = _jobs_c(self.jobs)
         o = _opts(mode, precision, polarization, stream=stream, use_graph=use_graph, ctas_per_sm=ctas_per_sm,
-                  first_hit=FIRST_HIT_TRAVERSE if first_hit is None else first_hit,
-                  blocks_per_item=blocks_per_item, autotune=autotune, node_width=node_width)
+                  first_hit=FIRST_HIT_AUTO if first_hit is None else first_hit,
+                  blocks_per_item=blocks_per_item, autotune=autotune, node_width=node_width, tile_cap=tile_cap)
         h = C.c_void_p()
         if isinstance(scene, Scene):
             check(lib().sbr_plan_create(scene.handle, self._jc, len(self.jobs), C.byref(o), C.byref(h)),
@@ -258,7 +260,7 @@ def _result(f, s, d, st, ms, npol):
 
 
 def run(scene: Scene, jobs: Sequence[JobSpec] | JobSpec, mode=MODE_BATCHED, precision=PREC_MIXED,
-        stream=None, first_hit=None, polarization=POL_SCALAR, blocks_per_item=0) -> SweepResult:
+        stream=None, first_hit=None, polarization=POL_SCALAR, blocks_per_item=0, tile_cap=0) -> SweepResult:
     """One call through sbr_run: host arrays in, host arrays out.  With
     polarization=POL_HHVV the fields, sigma and dBsm carry a trailing (HH, VV) axis."""
     if isinstance(jobs, JobSpec):
@@ -274,7 +276,8 @@ def run(scene: Scene, jobs: Sequence[JobSpec] | JobSpec, mode=MODE_BATCHED, prec
     r = _lib.Result()
     r.field, r.sigma_m2, r.rcs_dbsm, r.stats = f.ctypes.data, s.ctypes.data, d.ctypes.data, st.ctypes.data
     o = _opts(mode, precision, polarization, stream=stream,
-              first_hit=FIRST_HIT_TRAVERSE if first_hit is None else first_hit, blocks_per_item=blocks_per_item)
+              first_hit=FIRST_HIT_AUTO if first_hit is None else first_hit, blocks_per_item=blocks_per_item,
+              tile_cap=tile_cap)
     check(lib().sbr_run(scene.handle, jc, len(jobs), C.byref(r), C.byref(o)), "sbr_run")
     return _result(f, s, d, st.reshape(na, 4), r.device_ms, npol)
 
@@ -301,11 +304,12 @@ def adjoint(scene: Scene, jobs: Sequence[JobSpec] | JobSpec, cot, precision=PREC
     return gx.reshape(-1, 3), gf
 
 
-def trace_records(scene: Scene, job: JobSpec, precision=PREC_MIXED, first_hit=None) -> np.ndarray:
+def trace_records(scene: Scene, job: JobSpec, precision=PREC_MIXED, first_hit=None, tile_cap=0) -> np.ndarray:
     """Per-ray hit records [n_angles, ny, nx] (sbr_trace_records)."""
     jc = job.to_c()
     out = np.zeros((job.n_angles, job.ny, job.nx), dtype=RAY_RECORD)
-    o = _opts(MODE_BATCHED, precision, first_hit=FIRST_HIT_TRAVERSE if first_hit is None else first_hit)
+    o = _opts(MODE_BATCHED, precision, first_hit=FIRST_HIT_AUTO if first_hit is None else first_hit,
+              tile_cap=tile_cap)
     check(lib().sbr_trace_records(scene.handle, C.byref(jc), C.byref(o), _p(out)), "sbr_trace_records")
     return out
 

@@ -15,7 +15,7 @@ STATUS_NAMES = {
     12: "SBR_ERR_IO", 13: "SBR_ERR_PARSE", 14: "SBR_ERR_UNSUPPORTED",
 }
 MODE_BATCHED, MODE_PER_ANGLE = 0, 1
-FIRST_HIT_TRAVERSE, FIRST_HIT_RASTER = 0, 1
+FIRST_HIT_AUTO, FIRST_HIT_RASTER, FIRST_HIT_TRAVERSE = 0, 1, 2
 PREC_MIXED, PREC_FP32, PREC_FP64 = 0, 1, 2
 POL_SCALAR, POL_HHVV = 0, 1
 MAX_REC = 16
@@ -77,7 +77,8 @@ class RunOpts(C.Structure):
         ("blocks_per_item", C.c_int32),
         ("autotune", C.c_int32),
         ("node_width", C.c_int32),
-        ("reserved", C.c_int32 * 3),
+        ("tile_cap", C.c_int32),
+        ("reserved", C.c_int32 * 2),
     ]
 
 
@@ -106,6 +107,7 @@ class PlanInfo(C.Structure):
         ("blocks_per_item", C.c_int32),
         ("ctas_per_sm", C.c_int32),
         ("node_width", C.c_int32),
+        ("first_hit", C.c_int32),
     ]
 
 

@@ -110,13 +110,14 @@ struct __align__(16) Segment {
     int32_t blocks_x;     // ray blocks across the clipped rectangle
     int32_t blocks;       // blocks in the clipped rectangle
     int32_t blocks_per_item;
-    int32_t pad;
+    int32_t tbase;        // first-hit raster: first tile (ray block) of this segment within its chunk
     int64_t item_base;    // first work item of this segment
     int64_t sample_base;  // first output sample (angle, freq) index
     // pixel coordinates of a point P on the launcher grid: s = ps[0..2].P + ps[3],
     // t = pt[0..2].P + pt[3] (pixel (i, j) is centred at s = i, t = j)
     double ps[4], pt[4];
-    int64_t zbase;        // first first-hit buffer entry of this segment within its chunk
+    int64_t zbase;        // first first-hit buffer entry of this segment within its chunk (32 tbase;
+                          // entries are tile-major: tile, then lane of the 4 x 8 block)
 };
 // Per (job, angle) data of SBR_POL_HHVV plans: the transmit / receive unit vectors
 // e_H = phi-hat = (-sin phi, cos phi, 0) and e_V = theta-hat =

@@ -141,7 +141,7 @@ __device__ __forceinline__ void leaf_flag(const GTri* __restrict__ tris, int fir
                                           float tMin, float m, float dt, float& tBest, int& best, bool& amb) {
     for (int k = 0; k < cnt; ++k) {
         float tt;
-        if (wt_tri_flag<KZ>(tris[first + k], o, w, tMin, tBest, m, dt, tt, amb)) {
+        if (wt_tri_flag<KZ>(tris[first + k], o, w, tMin, tBest, m, dt, tt, amb) && replaces(tt, first + k, tBest, best)) {
             tBest = tt;
             best = first + k;
         }

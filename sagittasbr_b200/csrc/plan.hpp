@@ -94,14 +94,18 @@ struct sbr_plan {
     int64_t device_bytes = 0;
 
     // first-hit rasterisation: segments are processed in chunks whose first-hit
-    // buffers fit `d_zbuf`; each chunk = raster launch + trace launch
+    // buffers fit `d_zbuf`; each chunk = tile binning + tile raster + trace launch
     struct Chunk {
-        int64_t seg_begin, seg_end, item_begin, item_end, zcount;
+        int64_t seg_begin, seg_end, item_begin, item_end, zcount, tiles;
     };
     bool raster = false;
     std::vector<Chunk> chunks;
     unsigned long long* d_zbuf = nullptr;
     int64_t zbuf_elems = 0;
+    int64_t tiles_max = 0;              // tiles of the largest chunk
+    uint32_t tile_cap = 0;              // list entries per tile (longer lists walk)
+    uint32_t* d_tile_cnt = nullptr;     // [tiles_max]
+    int32_t* d_tile_list = nullptr;     // [tiles_max * tile_cap]
 
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaGraphExec_t graph = nullptr;
@@ -135,6 +139,7 @@ sbr_status build_tables(const sbr_scene* const* scenes, const int32_t* job_scene
                         size_t n_jobs, const sbr_run_opts& o, TableSink& sink, TableTotals& tot);
 
 sbr_status plan_launch(sbr_plan* pl, bool records, sbr_ray_record* d_records);
+
 sbr_status fill_records(sbr_ray_record* d, long long n, cudaStream_t st);
 // Traces the listed rays (angle index, i, j; checked by the caller) of a one-job plan.
 sbr_status trace_list_launch(sbr_plan* pl, const int32_t* d_rays, long long n, sbr_ray_record* d_out);

@@ -48,14 +48,8 @@ struct PolD {
 
 // PEC boundary condition: the reflected field is 2 (n.E) n - E (tangential part
 // reversed, normal part kept).
-__device__ __forceinline__ F3 pec_reflect(F3 e, F3 n) {
-    const float s = 2.0f * dot(n, e);
-    return f3(s * n.x - e.x, s * n.y - e.y, s * n.z - e.z);
-}
-__device__ __forceinline__ D3 pec_reflect(D3 e, D3 n) {
-    const double s = 2.0 * dot(n, e);
-    return D3{s * n.x - e.x, s * n.y - e.y, s * n.z - e.z};
-}
+__device__ __forceinline__ F3 pec_reflect(F3 e, F3 n) { return (2.0f * dot(n, e)) * n - e; }
+__device__ __forceinline__ D3 pec_reflect(D3 e, D3 n) { return (2.0 * dot(n, e)) * n - e; }
 
 // Co-polarised exit amplitude: 2 R^n e.(n x (d_in x E_in)), the direction of the PO
 // surface current n x H_in on the last surface projected on the receive
@@ -80,13 +74,13 @@ __device__ __forceinline__ F3 primary_origin(const Segment& G, const JobConst& J
     if (PREC == SBR_PREC_FP32) {
         const float u = __fdiv_rn(float(i) + 0.5f, float(J.nx));
         const float v = __fdiv_rn(float(j) + 0.5f, float(J.ny));
-        return f3(G.llcf[0] + u * G.uf[0] + v * G.vf[0], G.llcf[1] + u * G.uf[1] + v * G.vf[1],
-                  G.llcf[2] + u * G.uf[2] + v * G.vf[2]);
+        return f3(G.llcf[0], G.llcf[1], G.llcf[2]) + u * f3(G.uf[0], G.uf[1], G.uf[2]) +
+               v * f3(G.vf[0], G.vf[1], G.vf[2]);
     } else {
         const double u = (double(i) + 0.5) * J.inv_nx;
         const double v = (double(j) + 0.5) * J.inv_ny;
-        return f3(float(G.llc[0] + u * G.u[0] + v * G.v[0]), float(G.llc[1] + u * G.u[1] + v * G.v[1]),
-                  float(G.llc[2] + u * G.u[2] + v * G.v[2]));
+        const D3 o = D3{G.llc[0], G.llc[1], G.llc[2]} + u * D3{G.u[0], G.u[1], G.u[2]} + v * D3{G.v[0], G.v[1], G.v[2]};
+        return f3(float(o.x), float(o.y), float(o.z));
     }
 }
 
@@ -94,7 +88,8 @@ template <int PREC>
 __device__ __forceinline__ void start_f(RayF& r, const Segment& G, const JobConst& J, int i, int j) {
     r.o = primary_origin<PREC>(G, J, i, j);
     r.L = PREC == SBR_PREC_FP32 ? 0.0 : G.shift;
-    r.zidx = (int)(G.zbase + (int64_t)(j - G.j0) * G.ni + (i - G.i0));
+    const int bi = i - G.i0, bj = j - G.j0;
+    r.zidx = (int)(G.zbase + 32 * (int64_t)((bj >> 3) * G.blocks_x + (bi >> 2)) + ((bj & 7) << 2) + (bi & 3));
     r.d = f3(G.rdf[0], G.rdf[1], G.rdf[2]);
     r.nl = f3(0, 0, 0);
     r.dl = f3(0, 0, 0);
@@ -103,19 +98,23 @@ __device__ __forceinline__ void start_f(RayF& r, const Segment& G, const JobCons
     r.count = 0;
 }
 
+// First-hit buffer entries: (t bits << 32) | slot for a hit, kZMiss for none, and
+// kZWalk where the ray's first query walks the tree (its tile's triangle list was
+// too long to test); the high word of a hit is a finite positive float.
+constexpr unsigned long long kZMiss = ~0ull;
+constexpr unsigned long long kZWalk = 0xfffffffe00000000ull;
+
 // One closest-hit query, then reflect and nudge; true when the ray is finished.
-// The first query is read from the first-hit buffer when there is one (and the
-// entry is restored to empty for the next chunk).
+// The first query is read from the first-hit buffer when there is one.
 // SPEC: the speculative closest-hit walk, entered by all lanes of `mask` together.
 template <int PREC, bool REC, bool POL, bool W8 = false, bool SPEC = false>
 __device__ __forceinline__ bool step_f(RayF& r, PolF& e, const SceneView& S, int maxB, uint32_t& err,
                                        sbr_ray_record* rec, unsigned long long* zbuf, unsigned mask = 0u) {
     float tB = 1e20f;
     int slot;
-    if (zbuf != nullptr && r.count == 0) {
-        const unsigned long long key = zbuf[r.zidx];
-        zbuf[r.zidx] = ~0ull;
-        if (key == ~0ull) return true;
+    const unsigned long long key = (zbuf != nullptr && r.count == 0) ? zbuf[r.zidx] : kZWalk;
+    if (key == kZMiss) return true;
+    if (key != kZWalk) {
         tB = __uint_as_float((unsigned)(key >> 32));
         slot = (int)(unsigned)key;
     } else if constexpr (SPEC) {
@@ -171,8 +170,7 @@ __device__ __forceinline__ RayOut finish_f(const RayF& r, const JobConst& J) {
 __device__ __forceinline__ void start_d(RayD& r, const Segment& G, const JobConst& J, int i, int j) {
     const double u = (double(i) + 0.5) / double(J.nx);
     const double v = (double(j) + 0.5) / double(J.ny);
-    r.o = D3{G.llc[0] + u * G.u[0] + v * G.v[0], G.llc[1] + u * G.u[1] + v * G.v[1],
-             G.llc[2] + u * G.u[2] + v * G.v[2]};
+    r.o = D3{G.llc[0], G.llc[1], G.llc[2]} + u * D3{G.u[0], G.u[1], G.u[2]} + v * D3{G.v[0], G.v[1], G.v[2]};
     r.d = D3{-G.dir[0], -G.dir[1], -G.dir[2]};
     r.nl = D3{0, 0, 0};
     r.dl = D3{0, 0, 0};

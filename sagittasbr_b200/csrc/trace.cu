@@ -45,6 +45,7 @@ struct TraceParams {
     const volatile int32_t* cancel;
     sbr_ray_record* records;       // debug records (REC instantiation only)
     unsigned long long* zbuf;      // first-hit buffer of the launch's chunk, or null (walk the BVH)
+    const uint32_t* tile_cnt;      // with zbuf: triangles per tile of the chunk (0: every ray misses)
 };
 
 constexpr int kMaxK = 128;   // accumulation channels (frequencies x polarisations) per job
@@ -102,7 +103,7 @@ __device__ __forceinline__ void pol_finish_f(RayOut& o, const RayF& r, const Pol
     o.pa[0] = double(pol_amp(eh, r.nl, r.dl, e.h, twoRn));
     o.pa[1] = double(pol_amp(ev, r.nl, r.dl, e.v, twoRn));
     const F3 p = r.o - 1.0e-4f * r.nl;
-    o.Lp = r.L + P.plane - (G.dir[0] * double(p.x) + G.dir[1] * double(p.y) + G.dir[2] * double(p.z));
+    o.Lp = r.L + P.plane - dot(D3{G.dir[0], G.dir[1], G.dir[2]}, D3{double(p.x), double(p.y), double(p.z)});
     split_f32(0.5 * o.Lp, o.Lh, o.Ll);
 }
 __device__ __forceinline__ void pol_finish_d(RayOut& o, const RayD& r, const PolD& e, const SegPol& P,
@@ -233,6 +234,23 @@ __global__ void __launch_bounds__(kCtaThreads, min_ctas_per_sm<EPI>()) k_trace(c
             for (;;) {
                 const unsigned need = __ballot_sync(FULL, !active);
                 if (need == 0 || next >= nslots) break;
+                if (!REC && P.tile_cnt != nullptr && need == FULL) {
+                    // full blocks whose tile no triangle reaches: all 32 rays miss their
+                    // first query (counted as launched and queried, nothing else to do).
+                    // Only blocks inside the grid are skipped: the lanes a ragged block
+                    // leaves idle take the next block's first slots, and skipping it would
+                    // regroup the rays that follow into other FP32 partial sums.  So
+                    // `next` stays block-aligned here.
+                    while (next < nslots && (next & 31) == 0) {
+                        const int blk = b0 + (next >> 5);
+                        const int bi = (blk % G.blocks_x) * kBlockW, bj = (blk / G.blocks_x) * kBlockH;
+                        if (bi + kBlockW > G.ni || bj + kBlockH > G.nj || P.tile_cnt[G.tbase + blk] != 0u) break;
+                        ++cRays;
+                        ++cQuery;
+                        next += 32;
+                    }
+                    if (next >= nslots) break;
+                }
                 const int s = next + __popc(need & ((1u << lane) - 1u));
                 if (!active && s < nslots) {
                     const int blk = b0 + (s >> 5), l = s & 31;
@@ -500,86 +518,218 @@ __global__ void __launch_bounds__(128) k_trace_list(const TraceListParams P) {
 }
 
 // ------------------------------------------------------- first-hit raster
-struct RasterParams {
-    SceneView S;
+// Primary rays of one angle are parallel and start at the pixel centres of the
+// launcher grid, so the triangles a ray can hit first are those whose projection on
+// the launcher plane covers its pixel centre.  The raster bins the triangles to the
+// 4x8 ray tiles of the trace (one tile = the block of rays one warp traces) and tests
+// each tile's list with the trace's own watertight triangle test, one lane per ray,
+// as tile-based rasterisers do:
+//   k_tile_bin   lists, per tile, the triangles whose projection (widened by a
+//                margin) reaches the rectangle of the tile's pixel centres:
+//                projected box first, then the three edges; each tile holds up to
+//                `cap` triangles and counts the rest;
+//   k_tile_hit   the closest hit of every ray of a tile among its list (the walk's
+//                test, nearest t then lowest slot), written to the first-hit buffer
+//                as a hit key, kZMiss, or kZWalk for a tile with more than `cap`
+//                triangles.
+// The trace reads each ray's first query from the buffer; every other query walks.
+// Mixed precision only: the reference's Moller-Trumbore test of the FP32 mode is not
+// watertight, and near grazing incidence its hits can fall outside any margin around
+// the triangles' projections.
+struct TileParams {
+    const GTri* tris;
+    int32_t ntris;
+    uint32_t cap;                  // list entries per tile (longer lists: the rays walk)
     const Segment* segs;
     const JobConst* jobs;
-    int64_t seg_begin;        // first segment of the chunk (blockIdx.y counts from here)
-    int32_t ntris;
-    unsigned long long* zbuf; // [chunk pixels]: (float bits of t) << 32 | triangle slot, all ones = empty
+    int64_t seg_begin, seg_end;    // the chunk's segments
+    int64_t n_tiles;               // the chunk's tiles
+    uint32_t* cnt;                 // [n_tiles] triangles that reach each tile
+    int32_t* list;                 // [n_tiles * cap] triangle slots
+    unsigned long long* zbuf;      // [n_tiles * 32] first-hit entries, tile-major
 };
+constexpr int kBinThreads = 256;
 
-constexpr float kRasterMargin = 0.05f;  // pixels; covers FP32 rounding of ray origins and barycentrics
+// Margin (pixels) around a projected triangle: 0.06 pixel plus 2^-19 of the largest
+// launcher coordinate over the pixel size, which covers the FP32 rounding of the
+// ray origins, of the triangle test's sheared coordinates and of the edge test.
+__device__ __forceinline__ double tile_margin(const Segment& G, const JobConst& J) {
+    const double ext = fabs(G.llc[0]) + fabs(G.llc[1]) + fabs(G.llc[2]) + fabs(G.u[0]) + fabs(G.u[1]) +
+                       fabs(G.u[2]) + fabs(G.v[0]) + fabs(G.v[1]) + fabs(G.v[2]);
+    const double pu = sqrt(G.u[0] * G.u[0] + G.u[1] * G.u[1] + G.u[2] * G.u[2]) / J.nx;
+    const double pv = sqrt(G.v[0] * G.v[0] + G.v[1] * G.v[1] + G.v[2] * G.v[2]) / J.ny;
+    return 0.06 + ldexp(ext, -19) / fmin(pu, pv);
+}
 
-template <int PREC>
-__device__ __forceinline__ void raster_pixel(const GTri& T, int slot, const Segment& G, const JobConst& J, F3 d,
-                                             int i, int j, unsigned long long* zbuf) {
-    const F3 o = primary_origin<PREC>(G, J, i, j);
-    float t;
-    const bool hit = PREC == SBR_PREC_MIXED ? wt_f(T, o, wt_ray(d), 1.0e-3f, 1e20f, t) : mt_f(T, o, d, 1.0e-3f, 1e20f, t);
-    if (hit) {
-        const unsigned long long key = ((unsigned long long)__float_as_uint(t) << 32) | (unsigned)slot;
-        atomicMin(zbuf + G.zbase + (int64_t)(j - G.j0) * G.ni + (i - G.i0), key);
+// A triangle's footprint on one segment's pixel grid: the pixel-centre range of its
+// widened projected box (clipped to the segment), the tiles that range spans, and
+// its three edges as e(x, y) = ex (x - ilo) + ey (y - jlo) + ec >= 0 inside, in FP32
+// about the range's first pixel centre (widened by the margin; a projection of
+// near-zero area, or one within two tiles, keeps its box only: ex = ey = 0, ec = 1).
+struct TriFoot {
+    int ilo, ihi, jlo, jhi;
+    int bx0, by0, nbx, ntile;
+    int slot;
+    float ex[3], ey[3], ec[3];
+};
+__device__ __forceinline__ int tri_foot(const GTri& T, const Segment& G, double mg, int slot, TriFoot& f) {
+    const double X[3] = {T.v0.x, T.v1.x, T.v2.x};
+    const double Y[3] = {T.v0.y, T.v1.y, T.v2.y};
+    const double Z[3] = {T.v0.z, T.v1.z, T.v2.z};
+    double s[3], t[3];
+    double smin = 1e300, smax = -1e300, tmin = 1e300, tmax = -1e300;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        s[k] = G.ps[0] * X[k] + G.ps[1] * Y[k] + G.ps[2] * Z[k] + G.ps[3];
+        t[k] = G.pt[0] * X[k] + G.pt[1] * Y[k] + G.pt[2] * Z[k] + G.pt[3];
+        smin = fmin(smin, s[k]); smax = fmax(smax, s[k]);
+        tmin = fmin(tmin, t[k]); tmax = fmax(tmax, t[k]);
+    }
+    // (clamped to [-1, 2e9] before the conversions to int)
+    f.ilo = max(G.i0, (int)fmin(fmax(ceil(smin - mg), -1.0), 2.0e9));
+    f.ihi = min(G.i0 + G.ni - 1, (int)fmin(fmax(floor(smax + mg), -1.0), 2.0e9));
+    f.jlo = max(G.j0, (int)fmin(fmax(ceil(tmin - mg), -1.0), 2.0e9));
+    f.jhi = min(G.j0 + G.nj - 1, (int)fmin(fmax(floor(tmax + mg), -1.0), 2.0e9));
+    if (f.ihi < f.ilo || f.jhi < f.jlo) return 0;
+    f.slot = slot;
+    f.bx0 = (f.ilo - G.i0) >> 2;
+    f.by0 = (f.jlo - G.j0) >> 3;
+    f.nbx = ((f.ihi - G.i0) >> 2) - f.bx0 + 1;
+    f.ntile = f.nbx * (((f.jhi - G.j0) >> 3) - f.by0 + 1);
+    const double area2 = (s[1] - s[0]) * (t[2] - t[0]) - (t[1] - t[0]) * (s[2] - s[0]);
+    const bool edges = f.ntile > 2 && fabs(area2) >= 1e-6;
+    const double sg = area2 > 0.0 ? 1.0 : -1.0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int n = k == 2 ? 0 : k + 1;
+        const double ex = -sg * (t[n] - t[k]), ey = sg * (s[n] - s[k]);
+        f.ex[k] = edges ? float(ex) : 0.0f;
+        f.ey[k] = edges ? float(ey) : 0.0f;
+        f.ec[k] = edges ? float(ex * (f.ilo - s[k]) + ey * (f.jlo - t[k]) + mg * sqrt(ex * ex + ey * ey)) : 1.0f;
+    }
+    return f.ntile;
+}
+// Tile k of the footprint (row-major over its tile range) relative to the
+// segment's first tile, or -1 when an edge leaves every pixel centre of the tile
+// (inside the footprint's range) outside.
+__device__ __forceinline__ int foot_tile(const TriFoot& f, const Segment& G, int k) {
+    const int bx = f.bx0 + k % f.nbx, by = f.by0 + k / f.nbx;
+    const int x0 = max(G.i0 + kBlockW * bx, f.ilo) - f.ilo, x1 = min(G.i0 + kBlockW * bx + kBlockW - 1, f.ihi) - f.ilo;
+    const int y0 = max(G.j0 + kBlockH * by, f.jlo) - f.jlo, y1 = min(G.j0 + kBlockH * by + kBlockH - 1, f.jhi) - f.jlo;
+    const float cx = 0.5f * float(x0 + x1), cy = 0.5f * float(y0 + y1);
+    const float hx = 0.5f * float(x1 - x0), hy = 0.5f * float(y1 - y0);
+#pragma unroll
+    for (int e = 0; e < 3; ++e)
+        if (f.ex[e] * cx + f.ey[e] * cy + f.ec[e] + fabsf(f.ex[e]) * hx + fabsf(f.ey[e]) * hy < 0.0f) return -1;
+    return by * G.blocks_x + bx;
+}
+
+// One pass: every lane computes the footprint of its triangle into shared memory,
+// then the warp's (triangle, tile) pairs are dealt to its lanes 32 at a time (each
+// lane finds its pair's triangle by a binary search over the warp's prefix sums),
+// so footprints of any size keep every lane busy.
+__global__ void __launch_bounds__(kBinThreads) k_tile_bin(const TileParams P) {
+    constexpr unsigned FULL = 0xffffffffu;
+    __shared__ TriFoot s_foot[kBinThreads];
+    __shared__ int s_pre[kBinThreads];
+    const Segment& G = P.segs[P.seg_begin + blockIdx.y];
+    if (G.ni <= 0 || G.nj <= 0) return;
+    const double mg = tile_margin(G, P.jobs[G.job]);
+    const int lane = threadIdx.x & 31;
+    TriFoot* const wf = s_foot + (threadIdx.x & ~31);
+    int* const wp = s_pre + (threadIdx.x & ~31);
+    for (int base = blockIdx.x * blockDim.x; base < P.ntris; base += gridDim.x * blockDim.x) {
+        const int slot = base + threadIdx.x;
+        int nt = 0;
+        if (slot < P.ntris) nt = tri_foot(P.tris[slot], G, mg, slot, wf[lane]);
+        int pre = nt;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int y = __shfl_up_sync(FULL, pre, off);
+            if (lane >= off) pre += y;
+        }
+        wp[lane] = pre;
+        const int total = __shfl_sync(FULL, pre, 31);
+        __syncwarp();
+        for (int it = lane; it < total; it += 32) {
+            int lo = 0, hi = 31;  // the first lane whose inclusive prefix exceeds it
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (wp[mid] > it) hi = mid;
+                else lo = mid + 1;
+            }
+            const TriFoot& f = wf[lo];
+            const int b = foot_tile(f, G, it - (lo > 0 ? wp[lo - 1] : 0));
+            if (b < 0) continue;
+            const int64_t tile = G.tbase + (int64_t)b;
+            const uint32_t pos = atomicAdd(P.cnt + tile, 1u);
+            if (pos < P.cap) P.list[tile * P.cap + pos] = f.slot;
+        }
+        __syncwarp();
     }
 }
 
-// First closest hit of every primary ray of a chunk of segments.  Primary rays of
-// one angle are parallel and start at the pixel centres of the launcher grid, so a
-// triangle can only be hit by the rays whose pixel centres lie inside its projected
-// box (plus a small margin).  Each (segment, triangle) pair tests exactly those
-// rays with the trace's own triangle test (watertight in mixed precision,
-// Moller-Trumbore otherwise) and keeps, per pixel, the nearest hit
-// (smallest t, then smallest slot) with a 64-bit atomicMin.  Triangles covering
-// few pixels are done by one lane; larger ones are spread over the warp.
-template <int PREC>
-__global__ void __launch_bounds__(256) k_raster(const RasterParams R) {
+// The closest hit of each lane's ray among a tile's list: 32 triangles at a time,
+// each lane loading one (the loads overlap) and the warp handing their vertices
+// round, every lane testing every triangle.
+template <int KZ>
+__device__ __forceinline__ void tile_list_wt(const int32_t* list, uint32_t c, const GTri* tris, F3 o,
+                                             const WtRay& w, float& tB, int& best) {
     constexpr unsigned FULL = 0xffffffffu;
-    const Segment& G = R.segs[R.seg_begin + blockIdx.y];
-    if (G.ni <= 0 || G.nj <= 0) return;
-    const JobConst J = R.jobs[G.job];
-    const F3 d = f3(G.rdf[0], G.rdf[1], G.rdf[2]);
     const int lane = threadIdx.x & 31;
-    const int i_last = G.i0 + G.ni - 1, j_last = G.j0 + G.nj - 1;
-    for (int base = blockIdx.x * blockDim.x; base < R.ntris; base += gridDim.x * blockDim.x) {
-        const int slot = base + threadIdx.x;
-        int ilo = 1, ihi = 0, jlo = 1, jhi = 0;
-        GTri T;
-        if (slot < R.ntris) {
-            T = R.S.tris[slot];
-            const double X[3] = {T.v0.x, T.v1.x, T.v2.x};
-            const double Y[3] = {T.v0.y, T.v1.y, T.v2.y};
-            const double Z[3] = {T.v0.z, T.v1.z, T.v2.z};
-            double smin = 1e300, smax = -1e300, tmin = 1e300, tmax = -1e300;
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                const double s = G.ps[0] * X[k] + G.ps[1] * Y[k] + G.ps[2] * Z[k] + G.ps[3];
-                const double t = G.pt[0] * X[k] + G.pt[1] * Y[k] + G.pt[2] * Z[k] + G.pt[3];
-                smin = fmin(smin, s); smax = fmax(smax, s);
-                tmin = fmin(tmin, t); tmax = fmax(tmax, t);
+    for (uint32_t b = 0; b < c; b += 32) {
+        const int mine = b + lane < c ? list[b + lane] : 0;
+        const GTri M = tris[mine];
+        const int n = (int)min(32u, c - b);
+        for (int q = 0; q < n; ++q) {
+            const int slot = __shfl_sync(FULL, mine, q);
+            GTri T;
+            T.v0 = make_float4(__shfl_sync(FULL, M.v0.x, q), __shfl_sync(FULL, M.v0.y, q), __shfl_sync(FULL, M.v0.z, q), 0.0f);
+            T.v1 = make_float4(__shfl_sync(FULL, M.v1.x, q), __shfl_sync(FULL, M.v1.y, q), __shfl_sync(FULL, M.v1.z, q), 0.0f);
+            T.v2 = make_float4(__shfl_sync(FULL, M.v2.x, q), __shfl_sync(FULL, M.v2.y, q), __shfl_sync(FULL, M.v2.z, q), 0.0f);
+            float tt;
+            if (wt_tri<KZ>(T, o, w, 1.0e-3f, tB, tt) && replaces(tt, slot, tB, best)) {
+                tB = tt;
+                best = slot;
             }
-            ilo = max(G.i0, (int)fmax(ceil(smin - kRasterMargin), -1.0));
-            ihi = min(i_last, (int)fmin(floor(smax + kRasterMargin), 2.0e9));
-            jlo = max(G.j0, (int)fmax(ceil(tmin - kRasterMargin), -1.0));
-            jhi = min(j_last, (int)fmin(floor(tmax + kRasterMargin), 2.0e9));
         }
-        const int w = ihi - ilo + 1;
-        const int cnt = (ihi >= ilo && jhi >= jlo) ? w * (jhi - jlo + 1) : 0;
-        const bool big = cnt > 32;
-        if (!big) {
-            for (int jj = jlo; jj <= jhi; ++jj)
-                for (int ii = ilo; ii <= ihi; ++ii) raster_pixel<PREC>(T, slot, G, J, d, ii, jj, R.zbuf);
+    }
+}
+
+// One warp per tile (grid-stride): every lane's ray starts where the trace starts
+// it (primary_origin) and is tested as the trace's first query tests it.
+__global__ void __launch_bounds__(256) k_tile_hit(const TileParams P) {
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t t = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); t < P.n_tiles; t += nw) {
+        // the tile's segment: the last of the chunk whose first tile is <= t
+        int64_t lo = P.seg_begin, hi = P.seg_end - 1;
+        while (lo < hi) {
+            const int64_t mid = (lo + hi + 1) >> 1;
+            if (P.segs[mid].tbase <= t) lo = mid;
+            else hi = mid - 1;
         }
-        unsigned m = __ballot_sync(FULL, big);
-        while (m) {
-            const int src = __ffs(m) - 1;
-            m &= m - 1;
-            const int s_slot = __shfl_sync(FULL, slot, src);
-            const int s_ilo = __shfl_sync(FULL, ilo, src), s_jlo = __shfl_sync(FULL, jlo, src);
-            const int s_w = __shfl_sync(FULL, w, src), s_cnt = __shfl_sync(FULL, cnt, src);
-            const GTri Ts = R.S.tris[s_slot];
-            for (int c = lane; c < s_cnt; c += 32)
-                raster_pixel<PREC>(Ts, s_slot, G, J, d, s_ilo + c % s_w, s_jlo + c / s_w, R.zbuf);
+        const Segment& G = P.segs[lo];
+        const uint32_t c = P.cnt[t];
+        unsigned long long key = c > P.cap ? kZWalk : kZMiss;
+        if (c > 0 && c <= P.cap) {
+            const int blk = (int)(t - G.tbase);
+            const int i = G.i0 + (blk % G.blocks_x) * kBlockW + (lane % kBlockW);
+            const int j = G.j0 + (blk / G.blocks_x) * kBlockH + (lane / kBlockW);
+            const F3 o = primary_origin<SBR_PREC_MIXED>(G, P.jobs[G.job], i, j);
+            const WtRay w = wt_ray(f3(G.rdf[0], G.rdf[1], G.rdf[2]));
+            const int32_t* list = P.list + t * P.cap;
+            float tB = 1e20f;
+            int best = -1;
+            switch (w.kz) {
+                case 0: tile_list_wt<0>(list, c, P.tris, o, w, tB, best); break;
+                case 1: tile_list_wt<1>(list, c, P.tris, o, w, tB, best); break;
+                default: tile_list_wt<2>(list, c, P.tris, o, w, tB, best); break;
+            }
+            if (best >= 0 && i < G.i0 + G.ni && j < G.j0 + G.nj)
+                key = ((unsigned long long)__float_as_uint(tB) << 32) | (unsigned)best;
         }
+        P.zbuf[t * 32 + lane] = key;
     }
 }
 
@@ -705,6 +855,34 @@ void finalize(long long n_samples, int n_rep, const double* quantum, unsigned lo
 
 }  // namespace
 
+namespace {
+
+// Bins and rasterises the first hits of one chunk into the first-hit buffer.
+sbr_status tile_raster(sbr_plan* pl, const sbr_plan::Chunk& ch, cudaStream_t st, int& launches) {
+    TileParams t{};
+    t.tris = pl->scene_view.tris;
+    t.ntris = (int32_t)pl->scene->ntris;
+    t.cap = pl->tile_cap;
+    t.segs = pl->d_segs;
+    t.jobs = pl->d_jobs;
+    t.seg_begin = ch.seg_begin;
+    t.seg_end = ch.seg_end;
+    t.n_tiles = ch.tiles;
+    t.cnt = pl->d_tile_cnt;
+    t.list = pl->d_tile_list;
+    t.zbuf = pl->d_zbuf;
+    SBR_CUDA(cudaMemsetAsync(t.cnt, 0, (size_t)t.n_tiles * sizeof(uint32_t), st));
+    const unsigned gx = (unsigned)std::min<long long>((t.ntris + kBinThreads - 1) / kBinThreads, 4096);
+    k_tile_bin<<<dim3(gx, (unsigned)(t.seg_end - t.seg_begin)), kBinThreads, 0, st>>>(t);
+    const unsigned gh = (unsigned)std::min<long long>((t.n_tiles + 7) / 8, (long long)pl->num_sms * 64);
+    k_tile_hit<<<gh, 256, 0, st>>>(t);
+    launches += 2;
+    SBR_CUDA(cudaGetLastError());
+    return SBR_OK;
+}
+
+}  // namespace
+
 sbr_status plan_launch(sbr_plan* pl, bool records, sbr_ray_record* d_records) {
     const bool pol = pl->pol == SBR_POL_HHVV && !records;
     const int npol = pol ? 2 : 1;
@@ -734,26 +912,18 @@ sbr_status plan_launch(sbr_plan* pl, bool records, sbr_ray_record* d_records) {
             if (s != SBR_OK) return s;
         }
         if ((pl->mode == SBR_MODE_BATCHED || records) && pl->raster) {
-            // per chunk of segments: first hits by raster, then the persistent trace
-            const void* rfn = pl->prec == SBR_PREC_FP32 ? reinterpret_cast<const void*>(&k_raster<SBR_PREC_FP32>)
-                                                        : reinterpret_cast<const void*>(&k_raster<SBR_PREC_MIXED>);
+            // per chunk of segments: first hits by the tile raster, then the persistent trace
             p.k_begin = 0;
             p.k_count = 0;
             p.count_stats = 1;
             p.zbuf = pl->d_zbuf;
+            p.tile_cnt = pl->d_tile_cnt;
             for (size_t c = 0; c < pl->chunks.size(); ++c) {
                 const sbr_plan::Chunk& ch = pl->chunks[c];
-                RasterParams r{};
-                r.S = pl->scene_view;
-                r.segs = pl->d_segs;
-                r.jobs = pl->d_jobs;
-                r.seg_begin = ch.seg_begin;
-                r.ntris = (int32_t)pl->scene->ntris;
-                r.zbuf = pl->d_zbuf;
-                void* rargs[] = {&r};
-                const unsigned gx = (unsigned)std::min<long long>((pl->scene->ntris + 255) / 256, 4096);
-                SBR_CUDA(cudaLaunchKernel(rfn, dim3(gx, (unsigned)(ch.seg_end - ch.seg_begin)), dim3(256), rargs, 0, st));
-                ++launches;
+                if (ch.tiles > 0) {
+                    sbr_status s = tile_raster(pl, ch, st, launches);
+                    if (s != SBR_OK) return s;
+                }
                 if (ch.item_end > ch.item_begin) {
                     p.item_begin = ch.item_begin;
                     p.item_end = ch.item_end;

@@ -27,29 +27,50 @@ struct F3 {
 struct D3 {
     double x, y, z;
 };
+// The ray arithmetic is written with explicitly rounded operations (__fadd_rn,
+// __fmul_rn, ...: each rounded on its own, never contracted into a multiply-add),
+// so every kernel that starts, reflects or tests a ray -- the sweep in each of its
+// epilogue layouts, the record and ray-list traces, the first-hit raster, the error
+// bound's re-trace -- computes it bit for bit the same way.
 __device__ __forceinline__ F3 f3(float x, float y, float z) { return {x, y, z}; }
-__device__ __forceinline__ F3 operator+(F3 a, F3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
-__device__ __forceinline__ F3 operator-(F3 a, F3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
-__device__ __forceinline__ F3 operator*(float s, F3 a) { return {s * a.x, s * a.y, s * a.z}; }
-__device__ __forceinline__ float dot(F3 a, F3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ F3 operator+(F3 a, F3 b) {
+    return {__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z)};
+}
+__device__ __forceinline__ F3 operator-(F3 a, F3 b) {
+    return {__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y), __fsub_rn(a.z, b.z)};
+}
+__device__ __forceinline__ F3 operator*(float s, F3 a) { return {__fmul_rn(s, a.x), __fmul_rn(s, a.y), __fmul_rn(s, a.z)}; }
+__device__ __forceinline__ float dot(F3 a, F3 b) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fmul_rn(a.z, b.z));
+}
 __device__ __forceinline__ F3 cross(F3 a, F3 b) {
-    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+    return {__fsub_rn(__fmul_rn(a.y, b.z), __fmul_rn(a.z, b.y)), __fsub_rn(__fmul_rn(a.z, b.x), __fmul_rn(a.x, b.z)),
+            __fsub_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x))};
 }
 // Normalisation with the hardware reciprocal square root (a few ulp, like the
 // reference's --use_fast_math FP32 build).
 __device__ __forceinline__ F3 unit(F3 a) {
-    float r = rsqrtf(a.x * a.x + a.y * a.y + a.z * a.z);
-    return {a.x * r, a.y * r, a.z * r};
+    const float r = rsqrtf(dot(a, a));
+    return {__fmul_rn(a.x, r), __fmul_rn(a.y, r), __fmul_rn(a.z, r)};
 }
-__device__ __forceinline__ D3 operator+(D3 a, D3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
-__device__ __forceinline__ D3 operator-(D3 a, D3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
-__device__ __forceinline__ D3 operator*(double s, D3 a) { return {s * a.x, s * a.y, s * a.z}; }
-__device__ __forceinline__ double dot(D3 a, D3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ D3 operator+(D3 a, D3 b) {
+    return {__dadd_rn(a.x, b.x), __dadd_rn(a.y, b.y), __dadd_rn(a.z, b.z)};
+}
+__device__ __forceinline__ D3 operator-(D3 a, D3 b) {
+    return {__dsub_rn(a.x, b.x), __dsub_rn(a.y, b.y), __dsub_rn(a.z, b.z)};
+}
+__device__ __forceinline__ D3 operator*(double s, D3 a) {
+    return {__dmul_rn(s, a.x), __dmul_rn(s, a.y), __dmul_rn(s, a.z)};
+}
+__device__ __forceinline__ double dot(D3 a, D3 b) {
+    return __dadd_rn(__dadd_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y)), __dmul_rn(a.z, b.z));
+}
 __device__ __forceinline__ D3 cross(D3 a, D3 b) {
-    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+    return {__dsub_rn(__dmul_rn(a.y, b.z), __dmul_rn(a.z, b.y)), __dsub_rn(__dmul_rn(a.z, b.x), __dmul_rn(a.x, b.z)),
+            __dsub_rn(__dmul_rn(a.x, b.y), __dmul_rn(a.y, b.x))};
 }
 __device__ __forceinline__ D3 unit(D3 a) {
-    double l = sqrt(a.x * a.x + a.y * a.y + a.z * a.z);
+    const double l = sqrt(dot(a, a));
     return {a.x / l, a.y / l, a.z / l};
 }
 
@@ -185,7 +206,7 @@ __device__ __forceinline__ bool mt_f(const GTri& T, F3 o, F3 d, float tMin, floa
     if (u < 0.0f || u > 1.0f) return false;
     F3 qv = cross(tv, e1);
     float v = dot(d, qv) * inv;
-    if (v < 0.0f || u + v > 1.0f) return false;
+    if (v < 0.0f || __fadd_rn(u, v) > 1.0f) return false;
     float tt = dot(e2, qv) * inv;
     if (tt < tMin || tt > tMax) return false;
     t = tt;
@@ -261,6 +282,16 @@ __device__ __forceinline__ bool wt_tri(const GTri& T, F3 o, const WtRay& w, floa
     t = tt;
     return true;
 }
+// A hit at tt (<= tBest) of triangle `slot` replaces the closest one so far when it
+// is nearer, or as near with a lower slot (best = -1: none yet), so the closest hit
+// does not depend on the order triangles are tested in: the walk and the first-hit
+// raster pick the same triangle on exact ties.
+__device__ __forceinline__ bool replaces(float tt, int slot, float tBest, int best) {
+    return tt < tBest || (unsigned)slot < (unsigned)best;
+}
+__device__ __forceinline__ bool replaces(double tt, int slot, double tBest, int best) {
+    return tt < tBest || (unsigned)slot < (unsigned)best;
+}
 // A leaf's triangles with the axis order fixed at compile time: the switch on kz
 // sits outside the loop, so a warp whose rays share a dominant axis runs one variant.
 template <int KZ>
@@ -268,7 +299,7 @@ __device__ __forceinline__ void leaf_wt(const GTri* __restrict__ tris, int first
                                         float tMin, float& tBest, int& best) {
     for (int k = 0; k < cnt; ++k) {
         float tt;
-        if (wt_tri<KZ>(tris[first + k], o, w, tMin, tBest, tt)) {
+        if (wt_tri<KZ>(tris[first + k], o, w, tMin, tBest, tt) && replaces(tt, first + k, tBest, best)) {
             tBest = tt;
             best = first + k;
         }
@@ -293,7 +324,7 @@ __device__ __forceinline__ bool mt_d(const GTri64& T, D3 o, D3 d, double tMin, d
     if (u < 0.0 || u > 1.0) return false;
     D3 qv = cross(tv, e1);
     double v = dot(d, qv) * inv;
-    if (v < 0.0 || u + v > 1.0) return false;
+    if (v < 0.0 || __dadd_rn(u, v) > 1.0) return false;
     double tt = dot(e2, qv) * inv;
     if (tt < tMin || tt > tMax) return false;
     t = tt;
@@ -451,7 +482,10 @@ struct Walker<false> {
                 } else {
                     for (int k = 0; k < cnt; ++k) {
                         float tt;
-                        if (mt_f(S.tris[first + k], o, d, tMin, tBest, tt)) { tBest = tt; best = first + k; }
+                        if (mt_f(S.tris[first + k], o, d, tMin, tBest, tt) && replaces(tt, first + k, tBest, best)) {
+                            tBest = tt;
+                            best = first + k;
+                        }
                     }
                 }
                 if (!pop()) return best;
@@ -737,7 +771,10 @@ struct Walker<true> {
                 const int first = code >> 4, cnt = code & 15;
                 for (int k = 0; k < cnt; ++k) {
                     double tt;
-                    if (mt_d(S.tris64[first + k], o, d, tMin, tBest, tt)) { tBest = tt; best = first + k; }
+                    if (mt_d(S.tris64[first + k], o, d, tMin, tBest, tt) && replaces(tt, first + k, tBest, best)) {
+                        tBest = tt;
+                        best = first + k;
+                    }
                 }
                 if (!pop()) return best;
             } while (ref < 0);

@@ -68,7 +68,7 @@ def test_status_strings():
     for code, name in _lib.STATUS_NAMES.items():
         assert L.sbr_status_str(code).decode() == name
     assert L.sbr_status_str(999) == b"SBR_ERR_UNKNOWN"
-    assert L.sbr_abi_version() == 2
+    assert L.sbr_abi_version() == 3
 
 
 REF_STYLE_CONFIG = """# angular sampling
