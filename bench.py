@@ -338,7 +338,10 @@ def oracle_counts(w, n_angles: int = 8, per_angle: int = 512, threads: int = 0):
 #   aircraft: 8 of the 721 azimuths, 64 frequencies, one launch: 709.2 MB read +
 #             144.0 MB written for 4.253e8 queries;
 #   trihedral: 64 of the 8,281 angles, one launch: 4.82 MB + 1.25 MB for 2.96e7 queries.
-DRAM_BYTES_PER_QUERY = {"aircraft": 2.006, "trihedral": 0.205}
+# measured DRAM bytes (read + write) per closest-hit query of the sweep's kernels
+# (profiles/), by workload and first-hit mode: the raster adds the first-hit buffer
+# (8 B per ray, written and read) and the tile lists to the trace's own traffic
+DRAM_BYTES_PER_QUERY = {("aircraft", "walk"): 2.006, ("aircraft", "tile raster"): 15.20, ("trihedral", "walk"): 0.205}
 
 
 def hbm_peak_gbs() -> tuple[float, str]:
@@ -799,12 +802,15 @@ def main():
         vbox, vtri = counts["v_box"], counts["v_tri"]
         flop_q = FLOP_PER_BOX * vbox + FLOP_PER_TRI * vtri
         achieved = queries_all * flop_q / (kern_ms * 1e-3) / 1e12
-        dq = DRAM_BYTES_PER_QUERY.get(args.workload)
+        fh_name = {sbr.FIRST_HIT_RASTER: "tile raster", sbr.FIRST_HIT_TRAVERSE: "walk"}.get(info.get("first_hit"))
+        dq = DRAM_BYTES_PER_QUERY.get((args.workload, fh_name))
         hbm, hbm_src = hbm_peak_gbs()
         roof = {"bound": "fp32", "achieved": achieved, "peak": peak * ws, "unit": "TFLOP/s",
                 "frac": achieved / (peak * ws),
                 "traffic": dq * queries_all / ws if dq is not None else None,
-                "kernel": "k_trace (persistent) + k_finalize", "flop_per_query": flop_q, "v_box": vbox, "v_tri": vtri,
+                "kernel": ("k_tile_bin + k_tile_hit + k_trace (persistent) + k_finalize" if fh_name == "tile raster"
+                           else "k_trace (persistent) + k_finalize"),
+                "flop_per_query": flop_q, "v_box": vbox, "v_tri": vtri,
                 "queries_per_launch": queries_all / ws, "counts": counts,
                 "peak_source": "FP32 SGEMM 8192^3 measured in this run, per GPU (no FP32 figure in the peaks file)",
                 "fp32_fma_rate_at_sampled_clock": (fma_peak_tflops(torch, clk["sm_mhz"]) if clk else None),

@@ -113,9 +113,9 @@ __device__ __forceinline__ void adjoint_ray(const AdjointParams& P, const Segmen
         nLast = nn;
         dLast = d;
         L += t;
-        const D3 p = o + t * d;
-        d = unit(d - (2.0 * dot(d, nn)) * nn);
-        o = p + 1.0e-4 * nn;
+        const D3 p = fma3(t, d, o);
+        d = reflect_dir(d, nn);
+        o = nudge(p, nn);
     }
     const double cosT = -dot(nLast, dLast);
     if (!(cosT > 0.0)) return;  // the scalar gate: no term, no gradient
@@ -339,7 +339,7 @@ extern "C" sbr_status sbr_adjoint(sbr_scene* s, const sbr_job* jobs, size_t n_jo
     SBR_CUDA(cudaStreamSynchronize(stream));
     uint32_t e = 0;
     SBR_CUDA(cudaMemcpy(&e, s->d_err, sizeof(e), cudaMemcpyDeviceToHost));
-    if (e) SBR_CUDA(cudaMemset(s->d_err, 0, sizeof(e)));
+    if (e) clear_device_word(s->d_err);
     if (e & DEV_ERR_CANCEL) return fail(SBR_ERR_CANCELLED, "run cancelled");
     if (e & DEV_ERR_BUDGET) return fail(SBR_ERR_TIMEOUT, "traversal iteration budget exceeded");
     if (e & DEV_ERR_STACK) return fail(SBR_ERR_STACK, "traversal stack overflow");

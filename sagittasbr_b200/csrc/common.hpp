@@ -39,6 +39,16 @@ class DeviceGuard {
     int prev_ = -1;
 };
 
+// Zeroes one 32-bit device word before returning (a copy from pageable host memory
+// completes before cudaMemcpy returns; a cudaMemset would be queued on the legacy
+// stream, which the non-blocking streams the kernels run on do not wait for).
+template <class T>
+inline cudaError_t clear_device_word(T* d) {
+    static_assert(sizeof(T) == 4, "a 32-bit word");
+    const T zero = 0;
+    return cudaMemcpy(d, &zero, sizeof(T), cudaMemcpyHostToDevice);
+}
+
 // Device-side error word bits (written by kernels, read after each execute).
 enum : uint32_t {
     DEV_ERR_STACK = 1u,      // traversal stack would overflow (entry dropped)

@@ -252,10 +252,9 @@ __device__ __forceinline__ float ray_bound(const ErrParams& P, const Segment& G,
         r.dl = r.d;
         ++r.count;
         r.L += double(tB);
-        const F3 p = r.o + tB * r.d;
-        const float dn = 2.0f * dot(r.d, n);
-        r.d = unit(r.d - dn * n);
-        r.o = p + 1.0e-4f * n;
+        const F3 p = fma3(tB, r.d, r.o);
+        r.d = reflect_dir(r.d, n);
+        r.o = nudge(p, n);
         // uncertainty of this bounce
         const F3 e1 = f3(T.v1.x - T.v0.x, T.v1.y - T.v0.y, T.v1.z - T.v0.z);
         const F3 e2 = f3(T.v2.x - T.v0.x, T.v2.y - T.v0.y, T.v2.z - T.v0.z);
@@ -438,7 +437,7 @@ extern "C" sbr_status sbr_error_bound(sbr_scene* s, const sbr_job* jobs, size_t 
             e = cudaMemcpy(&de, p->d_err, sizeof(de), cudaMemcpyDeviceToHost);
             if (e != cudaSuccess) st = cuda_fail(e, "error word");
             else if (de) {
-                cudaMemset(p->d_err, 0, sizeof(de));
+                clear_device_word(p->d_err);
                 st = (de & DEV_ERR_CANCEL) ? fail(SBR_ERR_CANCELLED, "run cancelled")
                      : (de & DEV_ERR_BUDGET) ? fail(SBR_ERR_TIMEOUT, "traversal iteration budget exceeded")
                                              : fail(SBR_ERR_STACK, "traversal stack overflow");

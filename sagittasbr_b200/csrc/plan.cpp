@@ -68,12 +68,20 @@ sbr_status upload(T** d, const std::vector<T>& h, int64_t& bytes) {
 }
 
 template <class T>
-sbr_status zalloc(T** d, size_t count, int64_t& bytes) {
+sbr_status dalloc(T** d, size_t count, int64_t& bytes) {
     size_t n = std::max<size_t>(count, 1) * sizeof(T);
     cudaError_t e = cudaMalloc(d, n);
     if (e != cudaSuccess) return fail(SBR_ERR_OOM, "plan allocation failed");
     bytes += (int64_t)n;
-    SBR_CUDA(cudaMemset(*d, 0, n));
+    return SBR_OK;
+}
+// Zeroed on the plan's stream, so the plan's first launches come after the zeros
+// (a cudaMemset on the legacy stream is not ordered with a non-blocking stream).
+template <class T>
+sbr_status zalloc(T** d, size_t count, int64_t& bytes, cudaStream_t st) {
+    sbr_status r = dalloc(d, count, bytes);
+    if (r != SBR_OK) return r;
+    SBR_CUDA(cudaMemsetAsync(*d, 0, std::max<size_t>(count, 1) * sizeof(T), st));
     return SBR_OK;
 }
 
@@ -106,7 +114,7 @@ void release(sbr_plan* p) {
 sbr_status check_device_errors(sbr_plan* p) {
     uint32_t e = 0;
     SBR_CUDA(cudaMemcpy(&e, p->d_err, sizeof(e), cudaMemcpyDeviceToHost));
-    if (e) SBR_CUDA(cudaMemset(p->d_err, 0, sizeof(e)));
+    if (e) clear_device_word(p->d_err);
     if (e & DEV_ERR_CANCEL) return fail(SBR_ERR_CANCELLED, "run cancelled");
     if (e & DEV_ERR_BUDGET) return fail(SBR_ERR_TIMEOUT, "traversal iteration budget exceeded");
     if (e & DEV_ERR_STACK) return fail(SBR_ERR_STACK, "traversal stack overflow");
@@ -512,9 +520,9 @@ sbr_status plan_create(sbr_scene* const* scenes, size_t n_scenes, const int32_t*
     int64_t& b = p->device_bytes;
     if (p->raster) {
         // every entry of a chunk is written by its tile raster before the trace reads it
-        if ((st = zalloc(&p->d_zbuf, (size_t)p->zbuf_elems, b)) != SBR_OK ||
-            (st = zalloc(&p->d_tile_cnt, (size_t)p->tiles_max, b)) != SBR_OK ||
-            (st = zalloc(&p->d_tile_list, (size_t)p->tiles_max * p->tile_cap, b)) != SBR_OK) {
+        if ((st = dalloc(&p->d_zbuf, (size_t)p->zbuf_elems, b)) != SBR_OK ||
+            (st = dalloc(&p->d_tile_cnt, (size_t)p->tiles_max, b)) != SBR_OK ||
+            (st = dalloc(&p->d_tile_list, (size_t)p->tiles_max * p->tile_cap, b)) != SBR_OK) {
             release(p);
             return st;
         }
@@ -524,11 +532,11 @@ sbr_status plan_create(sbr_scene* const* scenes, size_t n_scenes, const int32_t*
         (st = upload(&p->d_quantum, p->quantum, b)) != SBR_OK ||
         (p->n_pol == 2 && (st = upload(&p->d_segpol, p->segpol, b)) != SBR_OK) ||
         (p->multi && (st = upload(&p->d_scenes, p->scene_views, b)) != SBR_OK) ||
-        (st = zalloc(&p->d_acc, 2 * (size_t)p->n_samples * p->n_pol * kAccReplicas, b)) != SBR_OK ||
-        (st = zalloc(&p->d_acc_stats, 4 * (size_t)p->n_segs, b)) != SBR_OK ||
-        (st = zalloc(&p->d_field, 2 * (size_t)p->n_samples * p->n_pol, b)) != SBR_OK ||
-        (st = zalloc(&p->d_stats, 4 * (size_t)p->n_segs, b)) != SBR_OK ||
-        (st = zalloc(&p->d_queue, 1 + (size_t)p->n_samples + p->chunks.size(), b)) != SBR_OK) {
+        (st = zalloc(&p->d_acc, 2 * (size_t)p->n_samples * p->n_pol * kAccReplicas, b, p->stream)) != SBR_OK ||
+        (st = zalloc(&p->d_acc_stats, 4 * (size_t)p->n_segs, b, p->stream)) != SBR_OK ||
+        (st = zalloc(&p->d_field, 2 * (size_t)p->n_samples * p->n_pol, b, p->stream)) != SBR_OK ||
+        (st = zalloc(&p->d_stats, 4 * (size_t)p->n_segs, b, p->stream)) != SBR_OK ||
+        (st = zalloc(&p->d_queue, 1 + (size_t)p->n_samples + p->chunks.size(), b, p->stream)) != SBR_OK) {
         release(p);
         return st;
     }

@@ -392,12 +392,12 @@ sbr_status sbr_scene_create(const float* xyz, size_t nverts, const uint32_t* tri
     if ((e = cudaMemcpy(s->d_nodes, g.data(), nb, cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(s->d_tris, tr.data(), tb, cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(s->d_tri_id, ids.data(), ib, cudaMemcpyHostToDevice)) != cudaSuccess ||
-        (e = cudaMemset(s->d_err, 0, sizeof(uint32_t))) != cudaSuccess)
+        (e = clear_device_word(s->d_err)) != cudaSuccess)
         return bail(cuda_fail(e, "scene upload"));
     // cancel flag: a device word (the kernels poll it from L2); the host sets it with an
     // asynchronous copy on a side stream, which runs while the sweep kernel is resident
     if ((e = cudaMalloc(&s->d_cancel, sizeof(int32_t))) != cudaSuccess ||
-        (e = cudaMemset(s->d_cancel, 0, sizeof(int32_t))) != cudaSuccess)
+        (e = clear_device_word(s->d_cancel)) != cudaSuccess)
         return bail(cuda_fail(e, "cancel flag"));
     if ((e = cudaHostAlloc(&s->h_flag_vals, 2 * sizeof(int32_t), cudaHostAllocDefault)) != cudaSuccess)
         return bail(cuda_fail(e, "cudaHostAlloc(cancel values)"));

@@ -102,7 +102,7 @@ __device__ __forceinline__ void pol_finish_f(RayOut& o, const RayF& r, const Pol
     const F3 ev = f3(float(P.ev[0]), float(P.ev[1]), float(P.ev[2]));
     o.pa[0] = double(pol_amp(eh, r.nl, r.dl, e.h, twoRn));
     o.pa[1] = double(pol_amp(ev, r.nl, r.dl, e.v, twoRn));
-    const F3 p = r.o - 1.0e-4f * r.nl;
+    const F3 p = fma3(-1.0e-4f, r.nl, r.o);
     o.Lp = r.L + P.plane - dot(D3{G.dir[0], G.dir[1], G.dir[2]}, D3{double(p.x), double(p.y), double(p.z)});
     split_f32(0.5 * o.Lp, o.Lh, o.Ll);
 }
@@ -115,7 +115,7 @@ __device__ __forceinline__ void pol_finish_d(RayOut& o, const RayD& r, const Pol
     const double twoRn = 2.0 * o.RnD;
     o.pa[0] = pol_amp(D3{P.eh[0], P.eh[1], P.eh[2]}, r.nl, r.dl, e.h, twoRn);
     o.pa[1] = pol_amp(D3{P.ev[0], P.ev[1], P.ev[2]}, r.nl, r.dl, e.v, twoRn);
-    const D3 p = r.o - 1.0e-4 * r.nl;
+    const D3 p = fma3(-1.0e-4, r.nl, r.o);
     o.Lp = r.L + P.plane - dot(D3{G.dir[0], G.dir[1], G.dir[2]}, p);
     split_f32(0.5 * o.Lp, o.Lh, o.Ll);
 }
@@ -1176,7 +1176,7 @@ extern "C" sbr_status sbr_run_noalloc(sbr_scene* s, const sbr_job* job, double* 
 
     uint32_t e = 0;
     SBR_CUDA(cudaMemcpy(&e, s->d_err, sizeof(e), cudaMemcpyDeviceToHost));
-    if (e) SBR_CUDA(cudaMemset(s->d_err, 0, sizeof(e)));
+    if (e) clear_device_word(s->d_err);
     if (e & DEV_ERR_CANCEL) return fail(SBR_ERR_CANCELLED, "run cancelled");
     if (e & DEV_ERR_BUDGET) return fail(SBR_ERR_TIMEOUT, "traversal iteration budget exceeded");
     if (e & DEV_ERR_STACK) return fail(SBR_ERR_STACK, "traversal stack overflow");

@@ -28,10 +28,11 @@ struct D3 {
     double x, y, z;
 };
 // The ray arithmetic is written with explicitly rounded operations (__fadd_rn,
-// __fmul_rn, ...: each rounded on its own, never contracted into a multiply-add),
-// so every kernel that starts, reflects or tests a ray -- the sweep in each of its
-// epilogue layouts, the record and ray-list traces, the first-hit raster, the error
-// bound's re-trace -- computes it bit for bit the same way.
+// __fmul_rn, __fmaf_rn, ...: each rounded once as written, never contracted or
+// split by the compiler), so every kernel that starts, reflects or tests a ray --
+// the sweep in each of its epilogue layouts, the record and ray-list traces, the
+// first-hit raster, the error bound's re-trace -- computes it bit for bit the same
+// way.  Products that are summed are fused (dot products, cross products, a s + b).
 __device__ __forceinline__ F3 f3(float x, float y, float z) { return {x, y, z}; }
 __device__ __forceinline__ F3 operator+(F3 a, F3 b) {
     return {__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z)};
@@ -40,12 +41,14 @@ __device__ __forceinline__ F3 operator-(F3 a, F3 b) {
     return {__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y), __fsub_rn(a.z, b.z)};
 }
 __device__ __forceinline__ F3 operator*(float s, F3 a) { return {__fmul_rn(s, a.x), __fmul_rn(s, a.y), __fmul_rn(s, a.z)}; }
-__device__ __forceinline__ float dot(F3 a, F3 b) {
-    return __fadd_rn(__fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fmul_rn(a.z, b.z));
+// s a + b, one rounding per component
+__device__ __forceinline__ F3 fma3(float s, F3 a, F3 b) {
+    return {__fmaf_rn(s, a.x, b.x), __fmaf_rn(s, a.y, b.y), __fmaf_rn(s, a.z, b.z)};
 }
+__device__ __forceinline__ float dot(F3 a, F3 b) { return __fmaf_rn(a.z, b.z, __fmaf_rn(a.y, b.y, __fmul_rn(a.x, b.x))); }
 __device__ __forceinline__ F3 cross(F3 a, F3 b) {
-    return {__fsub_rn(__fmul_rn(a.y, b.z), __fmul_rn(a.z, b.y)), __fsub_rn(__fmul_rn(a.z, b.x), __fmul_rn(a.x, b.z)),
-            __fsub_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x))};
+    return {__fmaf_rn(a.y, b.z, -__fmul_rn(a.z, b.y)), __fmaf_rn(a.z, b.x, -__fmul_rn(a.x, b.z)),
+            __fmaf_rn(a.x, b.y, -__fmul_rn(a.y, b.x))};
 }
 // Normalisation with the hardware reciprocal square root (a few ulp, like the
 // reference's --use_fast_math FP32 build).
@@ -62,12 +65,13 @@ __device__ __forceinline__ D3 operator-(D3 a, D3 b) {
 __device__ __forceinline__ D3 operator*(double s, D3 a) {
     return {__dmul_rn(s, a.x), __dmul_rn(s, a.y), __dmul_rn(s, a.z)};
 }
-__device__ __forceinline__ double dot(D3 a, D3 b) {
-    return __dadd_rn(__dadd_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y)), __dmul_rn(a.z, b.z));
+__device__ __forceinline__ D3 fma3(double s, D3 a, D3 b) {
+    return {__fma_rn(s, a.x, b.x), __fma_rn(s, a.y, b.y), __fma_rn(s, a.z, b.z)};
 }
+__device__ __forceinline__ double dot(D3 a, D3 b) { return __fma_rn(a.z, b.z, __fma_rn(a.y, b.y, __dmul_rn(a.x, b.x))); }
 __device__ __forceinline__ D3 cross(D3 a, D3 b) {
-    return {__dsub_rn(__dmul_rn(a.y, b.z), __dmul_rn(a.z, b.y)), __dsub_rn(__dmul_rn(a.z, b.x), __dmul_rn(a.x, b.z)),
-            __dsub_rn(__dmul_rn(a.x, b.y), __dmul_rn(a.y, b.x))};
+    return {__fma_rn(a.y, b.z, -__dmul_rn(a.z, b.y)), __fma_rn(a.z, b.x, -__dmul_rn(a.x, b.z)),
+            __fma_rn(a.x, b.y, -__dmul_rn(a.y, b.x))};
 }
 __device__ __forceinline__ D3 unit(D3 a) {
     const double l = sqrt(dot(a, a));
