@@ -341,7 +341,7 @@ def oracle_counts(w, n_angles: int = 8, per_angle: int = 512, threads: int = 0):
 # measured DRAM bytes (read + write) per closest-hit query of the sweep's kernels
 # (profiles/), by workload and first-hit mode: the raster adds the first-hit buffer
 # (8 B per ray, written and read) and the tile lists to the trace's own traffic
-DRAM_BYTES_PER_QUERY = {("aircraft", "walk"): 2.006, ("aircraft", "tile raster"): 15.20, ("trihedral", "walk"): 0.205}
+DRAM_BYTES_PER_QUERY = {("aircraft", "walk"): 2.006, ("aircraft", "tile raster"): 15.39, ("trihedral", "walk"): 0.205}
 
 
 def hbm_peak_gbs() -> tuple[float, str]:

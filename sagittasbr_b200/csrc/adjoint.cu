@@ -113,7 +113,7 @@ __device__ __forceinline__ void adjoint_ray(const AdjointParams& P, const Segmen
         nLast = nn;
         dLast = d;
         L += t;
-        const D3 p = fma3(t, d, o);
+        const D3 p = o + t * d;
         d = reflect_dir(d, nn);
         o = nudge(p, nn);
     }

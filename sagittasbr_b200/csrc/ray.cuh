@@ -49,14 +49,17 @@ struct PolD {
 // PEC boundary condition: the reflected field is 2 (n.E) n - E (tangential part
 // reversed, normal part kept).
 __device__ __forceinline__ F3 pec_reflect(F3 e, F3 n) { return fma3(2.0f * dot(n, e), n, f3(-e.x, -e.y, -e.z)); }
-__device__ __forceinline__ D3 pec_reflect(D3 e, D3 n) { return fma3(2.0 * dot(n, e), n, D3{-e.x, -e.y, -e.z}); }
+__device__ __forceinline__ D3 pec_reflect(D3 e, D3 n) {
+    const double s = 2.0 * dot(n, e);
+    return D3{s * n.x - e.x, s * n.y - e.y, s * n.z - e.z};
+}
 
 // Specular reflection of direction d at unit normal n, and the hit point p moved
 // off the surface along n: the bounce step of every FP32 / mixed and FP64 ray.
 __device__ __forceinline__ F3 reflect_dir(F3 d, F3 n) { return unit(fma3(-(2.0f * dot(d, n)), n, d)); }
-__device__ __forceinline__ D3 reflect_dir(D3 d, D3 n) { return unit(fma3(-(2.0 * dot(d, n)), n, d)); }
+__device__ __forceinline__ D3 reflect_dir(D3 d, D3 n) { return unit(d - (2.0 * dot(d, n)) * n); }
 __device__ __forceinline__ F3 nudge(F3 p, F3 n) { return fma3(1.0e-4f, n, p); }
-__device__ __forceinline__ D3 nudge(D3 p, D3 n) { return fma3(1.0e-4, n, p); }
+__device__ __forceinline__ D3 nudge(D3 p, D3 n) { return p + 1.0e-4 * n; }
 
 // Co-polarised exit amplitude: 2 R^n e.(n x (d_in x E_in)), the direction of the PO
 // surface current n x H_in on the last surface projected on the receive
@@ -176,7 +179,8 @@ __device__ __forceinline__ RayOut finish_f(const RayF& r, const JobConst& J) {
 __device__ __forceinline__ void start_d(RayD& r, const Segment& G, const JobConst& J, int i, int j) {
     const double u = (double(i) + 0.5) / double(J.nx);
     const double v = (double(j) + 0.5) / double(J.ny);
-    r.o = fma3(v, D3{G.v[0], G.v[1], G.v[2]}, fma3(u, D3{G.u[0], G.u[1], G.u[2]}, D3{G.llc[0], G.llc[1], G.llc[2]}));
+    r.o = D3{G.llc[0] + u * G.u[0] + v * G.v[0], G.llc[1] + u * G.u[1] + v * G.v[1],
+             G.llc[2] + u * G.u[2] + v * G.v[2]};
     r.d = D3{-G.dir[0], -G.dir[1], -G.dir[2]};
     r.nl = D3{0, 0, 0};
     r.dl = D3{0, 0, 0};
@@ -205,7 +209,7 @@ __device__ __forceinline__ bool step_d(RayD& r, PolD& e, const SceneView& S, int
     ++r.count;
     r.L += tB;
     if (REC && r.count <= SBR_MAX_REC) rec->tri[r.count - 1] = __ldg(S.tri_id + slot);
-    const D3 p = fma3(tB, r.d, r.o);
+    const D3 p = r.o + tB * r.d;
     r.d = reflect_dir(r.d, n);
     r.o = nudge(p, n);
     return r.count >= maxB;

@@ -115,7 +115,7 @@ __device__ __forceinline__ void pol_finish_d(RayOut& o, const RayD& r, const Pol
     const double twoRn = 2.0 * o.RnD;
     o.pa[0] = pol_amp(D3{P.eh[0], P.eh[1], P.eh[2]}, r.nl, r.dl, e.h, twoRn);
     o.pa[1] = pol_amp(D3{P.ev[0], P.ev[1], P.ev[2]}, r.nl, r.dl, e.v, twoRn);
-    const D3 p = fma3(-1.0e-4, r.nl, r.o);
+    const D3 p = r.o - 1.0e-4 * r.nl;
     o.Lp = r.L + P.plane - dot(D3{G.dir[0], G.dir[1], G.dir[2]}, p);
     split_f32(0.5 * o.Lp, o.Lh, o.Ll);
 }
@@ -670,25 +670,24 @@ __global__ void __launch_bounds__(kBinThreads) k_tile_bin(const TileParams P) {
 }
 
 // The closest hit of each lane's ray among a tile's list: 32 triangles at a time,
-// each lane loading one (the loads overlap) and the warp handing their vertices
-// round, every lane testing every triangle.
+// each lane loading one (the loads overlap) into the warp's slice of shared memory,
+// then every lane testing every triangle (broadcast reads).
 template <int KZ>
 __device__ __forceinline__ void tile_list_wt(const int32_t* list, uint32_t c, const GTri* tris, F3 o,
-                                             const WtRay& w, float& tB, int& best) {
-    constexpr unsigned FULL = 0xffffffffu;
+                                             const WtRay& w, float& tB, int& best, GTri* s_tri, int* s_slot) {
     const int lane = threadIdx.x & 31;
     for (uint32_t b = 0; b < c; b += 32) {
         const int mine = b + lane < c ? list[b + lane] : 0;
         const GTri M = tris[mine];
+        __syncwarp();  // the previous batch is read
+        s_tri[lane] = M;
+        s_slot[lane] = mine;
+        __syncwarp();
         const int n = (int)min(32u, c - b);
         for (int q = 0; q < n; ++q) {
-            const int slot = __shfl_sync(FULL, mine, q);
-            GTri T;
-            T.v0 = make_float4(__shfl_sync(FULL, M.v0.x, q), __shfl_sync(FULL, M.v0.y, q), __shfl_sync(FULL, M.v0.z, q), 0.0f);
-            T.v1 = make_float4(__shfl_sync(FULL, M.v1.x, q), __shfl_sync(FULL, M.v1.y, q), __shfl_sync(FULL, M.v1.z, q), 0.0f);
-            T.v2 = make_float4(__shfl_sync(FULL, M.v2.x, q), __shfl_sync(FULL, M.v2.y, q), __shfl_sync(FULL, M.v2.z, q), 0.0f);
+            const int slot = s_slot[q];
             float tt;
-            if (wt_tri<KZ>(T, o, w, 1.0e-3f, tB, tt) && replaces(tt, slot, tB, best)) {
+            if (wt_tri<KZ>(s_tri[q], o, w, 1.0e-3f, tB, tt) && replaces(tt, slot, tB, best)) {
                 tB = tt;
                 best = slot;
             }
@@ -699,7 +698,11 @@ __device__ __forceinline__ void tile_list_wt(const int32_t* list, uint32_t c, co
 // One warp per tile (grid-stride): every lane's ray starts where the trace starts
 // it (primary_origin) and is tested as the trace's first query tests it.
 __global__ void __launch_bounds__(256) k_tile_hit(const TileParams P) {
+    __shared__ GTri s_tri[256];
+    __shared__ int s_slot[256];
     const int lane = threadIdx.x & 31;
+    GTri* const wt = s_tri + (threadIdx.x & ~31);
+    int* const ws = s_slot + (threadIdx.x & ~31);
     const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
     for (int64_t t = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); t < P.n_tiles; t += nw) {
         // the tile's segment: the last of the chunk whose first tile is <= t
@@ -722,9 +725,9 @@ __global__ void __launch_bounds__(256) k_tile_hit(const TileParams P) {
             float tB = 1e20f;
             int best = -1;
             switch (w.kz) {
-                case 0: tile_list_wt<0>(list, c, P.tris, o, w, tB, best); break;
-                case 1: tile_list_wt<1>(list, c, P.tris, o, w, tB, best); break;
-                default: tile_list_wt<2>(list, c, P.tris, o, w, tB, best); break;
+                case 0: tile_list_wt<0>(list, c, P.tris, o, w, tB, best, wt, ws); break;
+                case 1: tile_list_wt<1>(list, c, P.tris, o, w, tB, best, wt, ws); break;
+                default: tile_list_wt<2>(list, c, P.tris, o, w, tB, best, wt, ws); break;
             }
             if (best >= 0 && i < G.i0 + G.ni && j < G.j0 + G.nj)
                 key = ((unsigned long long)__float_as_uint(tB) << 32) | (unsigned)best;

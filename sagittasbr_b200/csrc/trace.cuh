@@ -27,12 +27,13 @@ struct F3 {
 struct D3 {
     double x, y, z;
 };
-// The ray arithmetic is written with explicitly rounded operations (__fadd_rn,
-// __fmul_rn, __fmaf_rn, ...: each rounded once as written, never contracted or
-// split by the compiler), so every kernel that starts, reflects or tests a ray --
-// the sweep in each of its epilogue layouts, the record and ray-list traces, the
-// first-hit raster, the error bound's re-trace -- computes it bit for bit the same
-// way.  Products that are summed are fused (dot products, cross products, a s + b).
+// The FP32 / mixed ray arithmetic is written with explicitly rounded operations
+// (__fadd_rn, __fmul_rn, __fmaf_rn, ...: each rounded once as written, never
+// contracted or split by the compiler), so every kernel that starts, reflects or
+// tests a ray -- the sweep in each of its epilogue layouts, the record and ray-list
+// traces, the first-hit raster, the error bound's re-trace -- computes it bit for
+// bit the same way.  Products that are summed are fused (dot and cross products,
+// a s + b).
 __device__ __forceinline__ F3 f3(float x, float y, float z) { return {x, y, z}; }
 __device__ __forceinline__ F3 operator+(F3 a, F3 b) {
     return {__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z)};
@@ -56,25 +57,21 @@ __device__ __forceinline__ F3 unit(F3 a) {
     const float r = rsqrtf(dot(a, a));
     return {__fmul_rn(a.x, r), __fmul_rn(a.y, r), __fmul_rn(a.z, r)};
 }
-__device__ __forceinline__ D3 operator+(D3 a, D3 b) {
-    return {__dadd_rn(a.x, b.x), __dadd_rn(a.y, b.y), __dadd_rn(a.z, b.z)};
-}
-__device__ __forceinline__ D3 operator-(D3 a, D3 b) {
-    return {__dsub_rn(a.x, b.x), __dsub_rn(a.y, b.y), __dsub_rn(a.z, b.z)};
-}
-__device__ __forceinline__ D3 operator*(double s, D3 a) {
-    return {__dmul_rn(s, a.x), __dmul_rn(s, a.y), __dmul_rn(s, a.z)};
-}
+// FP64 vectors keep the compiler's plain evaluation, as the reference's USE_DOUBLE
+// build is compiled, so the FP64 mode reproduces that build's arithmetic; fma3 is
+// the explicitly fused form for the mixed-precision ray origins.
+__device__ __forceinline__ D3 operator+(D3 a, D3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ D3 operator-(D3 a, D3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ D3 operator*(double s, D3 a) { return {s * a.x, s * a.y, s * a.z}; }
 __device__ __forceinline__ D3 fma3(double s, D3 a, D3 b) {
     return {__fma_rn(s, a.x, b.x), __fma_rn(s, a.y, b.y), __fma_rn(s, a.z, b.z)};
 }
-__device__ __forceinline__ double dot(D3 a, D3 b) { return __fma_rn(a.z, b.z, __fma_rn(a.y, b.y, __dmul_rn(a.x, b.x))); }
+__device__ __forceinline__ double dot(D3 a, D3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 __device__ __forceinline__ D3 cross(D3 a, D3 b) {
-    return {__fma_rn(a.y, b.z, -__dmul_rn(a.z, b.y)), __fma_rn(a.z, b.x, -__dmul_rn(a.x, b.z)),
-            __fma_rn(a.x, b.y, -__dmul_rn(a.y, b.x))};
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
 }
 __device__ __forceinline__ D3 unit(D3 a) {
-    const double l = sqrt(dot(a, a));
+    double l = sqrt(a.x * a.x + a.y * a.y + a.z * a.z);
     return {a.x / l, a.y / l, a.z / l};
 }
 
@@ -328,7 +325,7 @@ __device__ __forceinline__ bool mt_d(const GTri64& T, D3 o, D3 d, double tMin, d
     if (u < 0.0 || u > 1.0) return false;
     D3 qv = cross(tv, e1);
     double v = dot(d, qv) * inv;
-    if (v < 0.0 || __dadd_rn(u, v) > 1.0) return false;
+    if (v < 0.0 || u + v > 1.0) return false;
     double tt = dot(e2, qv) * inv;
     if (tt < tMin || tt > tMax) return false;
     t = tt;
