@@ -94,12 +94,17 @@ __device__ __forceinline__ F3 primary_origin(const Segment& G, const JobConst& J
     }
 }
 
+// First-hit buffer entry of ray (i, j): tile-major, the lane of the 4x8 block last.
+__device__ __forceinline__ int zindex(const Segment& G, int i, int j) {
+    const int bi = i - G.i0, bj = j - G.j0;
+    return (int)(G.zbase + 32 * (int64_t)((bj >> 3) * G.blocks_x + (bi >> 2)) + ((bj & 7) << 2) + (bi & 3));
+}
+
 template <int PREC>
 __device__ __forceinline__ void start_f(RayF& r, const Segment& G, const JobConst& J, int i, int j) {
     r.o = primary_origin<PREC>(G, J, i, j);
     r.L = PREC == SBR_PREC_FP32 ? 0.0 : G.shift;
-    const int bi = i - G.i0, bj = j - G.j0;
-    r.zidx = (int)(G.zbase + 32 * (int64_t)((bj >> 3) * G.blocks_x + (bi >> 2)) + ((bj & 7) << 2) + (bi & 3));
+    r.zidx = zindex(G, i, j);
     r.d = f3(G.rdf[0], G.rdf[1], G.rdf[2]);
     r.nl = f3(0, 0, 0);
     r.dl = f3(0, 0, 0);
