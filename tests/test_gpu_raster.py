@@ -12,7 +12,9 @@ must equal the walking sweep's bit for bit:
 * the 199,808-triangle SH-displaced ellipsoid at its benchmark size (668^2 rays,
   4 bounces, 121 azimuths), with a graph-captured plan executed twice;
 * plans made before sbr_scene_update_vertices: the binning runs at every execution,
-  so a stretched mesh is binned as it is now.
+  so a stretched mesh is binned as it is now;
+* SBR_FIRST_HIT_AUTO (the default) rasterises a mixed-precision plan that launches at
+  least 8 rays per triangle per angle and walks otherwise (sbr_plan_info.first_hit).
 """
 import numpy as np
 import pytest
@@ -75,3 +77,20 @@ def test_raster_after_vertex_update():
         _same(pr.results(), pw.results())
         pr.close()
         pw.close()
+
+
+def test_auto_first_hit_choice():
+    dense_v, dense_t = M.box(1.0)  # 12 triangles, thousands of rays per angle
+    sparse_v, sparse_t = M.icosphere(3, 1.0)  # 1,280 triangles, 1,024 rays per angle
+    job_dense = sbr.JobSpec([90.0, 60.0], [0.0, 30.0], [3e9], 64, 64, 2.0, 3)
+    job_sparse = sbr.JobSpec([90.0, 60.0], [0.0, 30.0], [3e9], 32, 32, 2.2, 3)
+    with sbr.Scene(dense_v, dense_t) as sd, sbr.Scene(sparse_v, sparse_t) as ss:
+        for sc, job, want in ((sd, job_dense, sbr.FIRST_HIT_RASTER), (ss, job_sparse, sbr.FIRST_HIT_TRAVERSE)):
+            pl = sbr.Plan(sc, [job])
+            assert pl.info["first_hit"] == want
+            pl.execute()
+            _same(pl.results(), sbr.run(sc, job, first_hit=sbr.FIRST_HIT_TRAVERSE))
+            pl.close()
+        pl = sbr.Plan(sd, [job_dense], precision=sbr.PREC_FP32)
+        assert pl.info["first_hit"] == sbr.FIRST_HIT_TRAVERSE  # the raster is mixed precision only
+        pl.close()
