@@ -556,8 +556,9 @@ constexpr int kBinThreads = 256;
 __device__ __forceinline__ double tile_margin(const Segment& G, const JobConst& J) {
     const double ext = fabs(G.llc[0]) + fabs(G.llc[1]) + fabs(G.llc[2]) + fabs(G.u[0]) + fabs(G.u[1]) +
                        fabs(G.u[2]) + fabs(G.v[0]) + fabs(G.v[1]) + fabs(G.v[2]);
-    const double pu = sqrt(G.u[0] * G.u[0] + G.u[1] * G.u[1] + G.u[2] * G.u[2]) / J.nx;
-    const double pv = sqrt(G.v[0] * G.v[0] + G.v[1] * G.v[1] + G.v[2] * G.v[2]) / J.ny;
+    // pixel sizes from FP32 square roots rounded down (only a larger margin results)
+    const double pu = double(sqrtf(float(G.u[0] * G.u[0] + G.u[1] * G.u[1] + G.u[2] * G.u[2])) * 0.999999f) / J.nx;
+    const double pv = double(sqrtf(float(G.v[0] * G.v[0] + G.v[1] * G.v[1] + G.v[2] * G.v[2])) * 0.999999f) / J.ny;
     return 0.06 + ldexp(ext, -19) / fmin(pu, pv);
 }
 
@@ -605,7 +606,9 @@ __device__ __forceinline__ int tri_foot(const GTri& T, const Segment& G, double 
         const double ex = -sg * (t[n] - t[k]), ey = sg * (s[n] - s[k]);
         f.ex[k] = edges ? float(ex) : 0.0f;
         f.ey[k] = edges ? float(ey) : 0.0f;
-        f.ec[k] = edges ? float(ex * (f.ilo - s[k]) + ey * (f.jlo - t[k]) + mg * sqrt(ex * ex + ey * ey)) : 1.0f;
+        // |(ex, ey)| from an FP32 square root rounded up: the margin only widens
+        const double len = double(sqrtf(float(ex * ex + ey * ey)) * 1.000001f);
+        f.ec[k] = edges ? float(ex * (f.ilo - s[k]) + ey * (f.jlo - t[k]) + mg * len) : 1.0f;
     }
     return f.ntile;
 }
