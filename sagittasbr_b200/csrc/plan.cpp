@@ -520,11 +520,29 @@ sbr_status plan_create(sbr_scene* const* scenes, size_t n_scenes, const int32_t*
     int64_t& b = p->device_bytes;
     if (p->raster) {
         // every entry of a chunk is written by its tile raster before the trace reads it
+        const int64_t b0 = b;
         if ((st = dalloc(&p->d_zbuf, (size_t)p->zbuf_elems, b)) != SBR_OK ||
             (st = dalloc(&p->d_tile_cnt, (size_t)p->tiles_max, b)) != SBR_OK ||
             (st = dalloc(&p->d_tile_list, (size_t)p->tiles_max * p->tile_cap, b)) != SBR_OK) {
-            release(p);
-            return st;
+            if (o.first_hit == SBR_FIRST_HIT_RASTER) {
+                release(p);
+                return st;
+            }
+            // chosen automatically: without room for its buffers the plan walks instead
+            // (a failed cudaMalloc is not sticky; its error is cleared here)
+            cudaGetLastError();
+            cudaFree(p->d_zbuf);
+            cudaFree(p->d_tile_cnt);
+            cudaFree(p->d_tile_list);
+            p->d_zbuf = nullptr;
+            p->d_tile_cnt = nullptr;
+            p->d_tile_list = nullptr;
+            b = b0;
+            p->raster = false;
+            p->chunks.clear();
+            p->zbuf_elems = 0;
+            p->tiles_max = 0;
+            st = SBR_OK;
         }
     }
     if ((st = upload(&p->d_segs, p->segs, b)) != SBR_OK || (st = upload(&p->d_seg_base, p->seg_base, b)) != SBR_OK ||
