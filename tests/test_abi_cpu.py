@@ -62,6 +62,24 @@ def test_struct_layouts_match_header(tmp_path):
     assert got["sbr_ray_record"] == sbr.RAY_RECORD.itemsize
 
 
+def test_constants_match_header(tmp_path):
+    """The ctypes mirror's mode, precision, polarisation and first-hit constants are
+    the header's."""
+    names = ["SBR_MODE_BATCHED", "SBR_MODE_PER_ANGLE", "SBR_PREC_MIXED", "SBR_PREC_FP32", "SBR_PREC_FP64",
+             "SBR_POL_SCALAR", "SBR_POL_HHVV", "SBR_FIRST_HIT_AUTO", "SBR_FIRST_HIT_RASTER",
+             "SBR_FIRST_HIT_TRAVERSE"]
+    lines = ['#include <stdio.h>', '#include "sbr.h"', "int main(void){"]
+    lines += [f'printf("%d\\n", (int){n});' for n in names]
+    lines.append("return 0; }")
+    src = tmp_path / "consts.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "consts"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    want = [getattr(_lib, n[4:]) for n in names]
+    assert got == want
+
+
 def test_status_strings():
     L = _lib.lib()
     assert L.sbr_status_str(0) == b"SBR_OK"
