@@ -5,7 +5,9 @@ procedural aircraft of 2,148,800 triangles (superellipsoid fuselage 20 m x 1.5 m
 swept trapezoidal wings of 18 m span and 3 -> 1 m chord, tail; Gaussian vertex jitter
 1 mm), 64 frequencies log-spaced over 1-18 GHz, 721 azimuths at 0.5 deg (theta = 90),
 max 5 bounces, 10 rays per wavelength over the bounding aperture (G = 20.36 m; all
-frequencies share one trace on the 12,222^2 grid of 18 GHz), one persistent launch.
+frequencies share one trace on the 12,222^2 grid of 18 GHz); the primary rays' first
+hits come from the tile-binned raster (the plan's automatic choice for this dense
+sweep), every later bounce from the persistent trace, chunk by chunk of angles.
 Other workloads (--workload): `trihedral` (3 x 100x100x2 triangles, 10 GHz, 578^2
 rays, 3 bounces, theta, phi = 0..90 at 1 deg = 8,281 angles), `sphere` (icosphere
 level 5, 1 GHz, 67^2 rays, 3 bounces, 360 azimuths), `aircraft-dev` (8 frequencies x
