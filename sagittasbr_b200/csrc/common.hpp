@@ -101,6 +101,7 @@ struct SceneView {
     const GTri64* __restrict__ tris64;
     const int32_t* __restrict__ tri_id;
     const GNode8* __restrict__ nodes8;  // the 8-wide tree of the same leaves, or null
+    const int32_t* __restrict__ tie;    // per slot: rank in the reference's walk order, or null
 };
 
 // --------------------------------------------------------------- plan data

@@ -137,11 +137,13 @@ __device__ __forceinline__ bool wt_tri_flag(const GTri& T, F3 o, const WtRay& w,
 }
 
 template <int KZ>
-__device__ __forceinline__ void leaf_flag(const GTri* __restrict__ tris, int first, int cnt, F3 o, const WtRay& w,
-                                          float tMin, float m, float dt, float& tBest, int& best, bool& amb) {
+__device__ __forceinline__ void leaf_flag(const GTri* __restrict__ tris, const int32_t* tie, int first, int cnt, F3 o,
+                                          const WtRay& w, float tMin, float m, float dt, float& tBest, int& best,
+                                          bool& amb) {
     for (int k = 0; k < cnt; ++k) {
         float tt;
-        if (wt_tri_flag<KZ>(tris[first + k], o, w, tMin, tBest, m, dt, tt, amb) && replaces(tt, first + k, tBest, best)) {
+        if (wt_tri_flag<KZ>(tris[first + k], o, w, tMin, tBest, m, dt, tt, amb) &&
+            replaces(tt, first + k, tBest, best, tie)) {
             tBest = tt;
             best = first + k;
         }
@@ -203,9 +205,9 @@ __device__ int closest_flag(const SceneView& S, F3 o, F3 d, float tMin, float& t
                 const int code = ~ref;
                 const int first = code >> 4, cnt = code & 15;
                 switch (wr.kz) {
-                    case 0: leaf_flag<0>(S.tris, first, cnt, o, wr, tMin, m, dt, tBest, best, amb); break;
-                    case 1: leaf_flag<1>(S.tris, first, cnt, o, wr, tMin, m, dt, tBest, best, amb); break;
-                    default: leaf_flag<2>(S.tris, first, cnt, o, wr, tMin, m, dt, tBest, best, amb); break;
+                    case 0: leaf_flag<0>(S.tris, S.tie, first, cnt, o, wr, tMin, m, dt, tBest, best, amb); break;
+                    case 1: leaf_flag<1>(S.tris, S.tie, first, cnt, o, wr, tMin, m, dt, tBest, best, amb); break;
+                    default: leaf_flag<2>(S.tris, S.tie, first, cnt, o, wr, tMin, m, dt, tBest, best, amb); break;
                 }
                 ref = -1;
                 while (sp > 0) {

@@ -28,6 +28,7 @@ struct sbr_scene {
     sbr::GTri* d_tris = nullptr;
     sbr::GTri64* d_tris64 = nullptr;
     int32_t* d_tri_id = nullptr;
+    int32_t* d_tie = nullptr;        // exact-tie ranks (coincident faces of opposite winding), or null
     float* d_xyz = nullptr;          // caller vertices and triangles, uploaded for the adjoint
     uint32_t* d_idx = nullptr;
     uint32_t* d_err = nullptr;
@@ -45,7 +46,7 @@ struct sbr_scene {
     float* d_tri_box = nullptr;
     int64_t device_bytes = 0;
 
-    sbr::SceneView view() const { return sbr::SceneView{d_nodes, d_tris, d_tris64, d_tri_id, d_nodes8}; }
+    sbr::SceneView view() const { return sbr::SceneView{d_nodes, d_tris, d_tris64, d_tri_id, d_nodes8, d_tie}; }
 };
 
 struct sbr_plan {

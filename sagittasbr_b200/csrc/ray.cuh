@@ -201,7 +201,9 @@ __device__ __forceinline__ bool step_d(RayD& r, PolD& e, const SceneView& S, int
     const int slot = Walker<true>::closest(S, r.o, r.d, 1.0e-3, tB, err);
     if (slot < 0) return true;
     const GTri64& T = S.tris64[slot];
-    const D3 n{T.n[0], T.n[1], T.n[2]};
+    // the hit normal unit(e1 x e2) formed here, as the reference forms it on the
+    // device for every hit (src/cuda/rtKernels.cu:42), not the host's copy
+    const D3 n = unit(cross(D3{T.e1[0], T.e1[1], T.e1[2]}, D3{T.e2[0], T.e2[1], T.e2[2]}));
     if constexpr (POL) {
         if (r.count > 0) {
             e.h = pec_reflect(e.h, r.nl);

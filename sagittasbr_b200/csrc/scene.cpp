@@ -11,6 +11,7 @@
 
 #include "bvh_build.hpp"
 #include "plan.hpp"
+#include "tie_order.hpp"
 
 using namespace sbr;
 
@@ -68,6 +69,7 @@ void free_scene(sbr_scene* s) {
     cudaFree(s->d_tris);
     cudaFree(s->d_tris64);
     cudaFree(s->d_tri_id);
+    cudaFree(s->d_tie);
     cudaFree(s->d_xyz);
     cudaFree(s->d_idx);
     cudaFree(s->d_refit_nodes);
@@ -377,6 +379,15 @@ sbr_status sbr_scene_create(const float* xyz, size_t nverts, const uint32_t* tri
             tr[slot].v2 = make_float4(c[0], c[1], c[2], n[2]);
         }
     });
+    // exact ties: where the mesh holds a triangle twice with opposite windings, each
+    // slot's rank in the reference's walk order decides which of two equally near
+    // triangles a ray keeps (the reference keeps the last it tests)
+    std::vector<int32_t> tie;
+    if (has_opposed_twins(xyz, tri_idx, ntris)) {
+        const std::vector<int32_t> rank = reference_walk_rank(xyz, tri_idx, ntris, scale, o.n_threads);
+        tie.resize(ntris);
+        for (size_t slot = 0; slot < ntris; ++slot) tie[slot] = rank[(size_t)s->order[slot]];
+    }
     auto t1 = std::chrono::steady_clock::now();
     s->build_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
 
@@ -407,6 +418,13 @@ sbr_status sbr_scene_create(const float* xyz, size_t nverts, const uint32_t* tri
         (e = cudaStreamCreateWithFlags(&s->cancel_stream, cudaStreamNonBlocking)) != cudaSuccess)
         return bail(cuda_fail(e, "cudaStreamCreate"));
     s->device_bytes = (int64_t)(nb + tb + ib);
+    if (!tie.empty()) {
+        if ((e = cudaMalloc(&s->d_tie, ib)) != cudaSuccess)
+            return bail(fail(SBR_ERR_OOM, std::string("device allocation failed: ") + cudaGetErrorString(e)));
+        if ((e = cudaMemcpy(s->d_tie, tie.data(), ib, cudaMemcpyHostToDevice)) != cudaSuccess)
+            return bail(cuda_fail(e, "tie rank upload"));
+        s->device_bytes += (int64_t)ib;
+    }
     if (!g8.empty()) {
         const size_t nb8 = sizeof(GNode8) * g8.size();
         if ((e = cudaMalloc(&s->d_nodes8, nb8)) != cudaSuccess)

@@ -538,6 +538,7 @@ __global__ void __launch_bounds__(128) k_trace_list(const TraceListParams P) {
 // the triangles' projections.
 struct TileParams {
     const GTri* tris;
+    const int32_t* tie;            // exact-tie ranks of the scene, or null
     int32_t ntris;
     uint32_t cap;                  // list entries per tile (longer lists: the rays walk)
     const Segment* segs;
@@ -676,8 +677,8 @@ __global__ void __launch_bounds__(kBinThreads) k_tile_bin(const TileParams P) {
 // each lane loading one (the loads overlap) into the warp's slice of shared memory,
 // then every lane testing every triangle (broadcast reads).
 template <int KZ>
-__device__ __forceinline__ void tile_list_wt(const int32_t* list, uint32_t c, const GTri* tris, F3 o,
-                                             const WtRay& w, float& tB, int& best, GTri* s_tri, int* s_slot) {
+__device__ __forceinline__ void tile_list_wt(const int32_t* list, uint32_t c, const GTri* tris, const int32_t* tie,
+                                             F3 o, const WtRay& w, float& tB, int& best, GTri* s_tri, int* s_slot) {
     const int lane = threadIdx.x & 31;
     for (uint32_t b = 0; b < c; b += 32) {
         const int mine = b + lane < c ? list[b + lane] : 0;
@@ -690,7 +691,7 @@ __device__ __forceinline__ void tile_list_wt(const int32_t* list, uint32_t c, co
         for (int q = 0; q < n; ++q) {
             const int slot = s_slot[q];
             float tt;
-            if (wt_tri<KZ>(s_tri[q], o, w, 1.0e-3f, tB, tt) && replaces(tt, slot, tB, best)) {
+            if (wt_tri<KZ>(s_tri[q], o, w, 1.0e-3f, tB, tt) && replaces(tt, slot, tB, best, tie)) {
                 tB = tt;
                 best = slot;
             }
@@ -728,9 +729,9 @@ __global__ void __launch_bounds__(256) k_tile_hit(const TileParams P) {
             float tB = 1e20f;
             int best = -1;
             switch (w.kz) {
-                case 0: tile_list_wt<0>(list, c, P.tris, o, w, tB, best, wt, ws); break;
-                case 1: tile_list_wt<1>(list, c, P.tris, o, w, tB, best, wt, ws); break;
-                default: tile_list_wt<2>(list, c, P.tris, o, w, tB, best, wt, ws); break;
+                case 0: tile_list_wt<0>(list, c, P.tris, P.tie, o, w, tB, best, wt, ws); break;
+                case 1: tile_list_wt<1>(list, c, P.tris, P.tie, o, w, tB, best, wt, ws); break;
+                default: tile_list_wt<2>(list, c, P.tris, P.tie, o, w, tB, best, wt, ws); break;
             }
             if (best >= 0 && i < G.i0 + G.ni && j < G.j0 + G.nj)
                 key = ((unsigned long long)__float_as_uint(tB) << 32) | (unsigned)best;
@@ -867,6 +868,7 @@ namespace {
 sbr_status tile_raster(sbr_plan* pl, const sbr_plan::Chunk& ch, cudaStream_t st, int& launches) {
     TileParams t{};
     t.tris = pl->scene_view.tris;
+    t.tie = pl->scene_view.tie;
     t.ntris = (int32_t)pl->scene->ntris;
     t.cap = pl->tile_cap;
     t.segs = pl->d_segs;

@@ -67,8 +67,10 @@ __device__ __forceinline__ D3 fma3(double s, D3 a, D3 b) {
     return {__fma_rn(s, a.x, b.x), __fma_rn(s, a.y, b.y), __fma_rn(s, a.z, b.z)};
 }
 __device__ __forceinline__ double dot(D3 a, D3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+// written as the reference's vec3 cross (include/RT/vec3.h:115-119), y negated, so
+// the compiler fuses the same products
 __device__ __forceinline__ D3 cross(D3 a, D3 b) {
-    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+    return {a.y * b.z - a.z * b.y, -(a.x * b.z - a.z * b.x), a.x * b.y - a.y * b.x};
 }
 __device__ __forceinline__ D3 unit(D3 a) {
     double l = sqrt(a.x * a.x + a.y * a.y + a.z * a.z);
@@ -284,23 +286,29 @@ __device__ __forceinline__ bool wt_tri(const GTri& T, F3 o, const WtRay& w, floa
     return true;
 }
 // A hit at tt (<= tBest) of triangle `slot` replaces the closest one so far when it
-// is nearer, or as near with a lower slot (best = -1: none yet), so the closest hit
-// does not depend on the order triangles are tested in: the walk and the first-hit
-// raster pick the same triangle on exact ties.
-__device__ __forceinline__ bool replaces(float tt, int slot, float tBest, int best) {
-    return tt < tBest || (unsigned)slot < (unsigned)best;
+// is nearer, or none is kept yet (best = -1), or it is as near and comes later in
+// the tie order: the rank of the triangle in the reference's walk (tie[slot]; the
+// reference keeps the last of equally near triangles), or, where the scene stores
+// no ranks (no coincident faces of opposite winding), the slot order reversed.  The
+// closest hit does not depend on the order triangles are tested in, so the walk and
+// the first-hit raster keep the same triangle on exact ties.
+__device__ __forceinline__ bool tie_later(int slot, int best, const int32_t* __restrict__ tie) {
+    return tie ? __ldg(tie + slot) > __ldg(tie + best) : slot < best;
 }
-__device__ __forceinline__ bool replaces(double tt, int slot, double tBest, int best) {
-    return tt < tBest || (unsigned)slot < (unsigned)best;
+__device__ __forceinline__ bool replaces(float tt, int slot, float tBest, int best, const int32_t* tie) {
+    return tt < tBest || best < 0 || tie_later(slot, best, tie);
+}
+__device__ __forceinline__ bool replaces(double tt, int slot, double tBest, int best, const int32_t* tie) {
+    return tt < tBest || best < 0 || tie_later(slot, best, tie);
 }
 // A leaf's triangles with the axis order fixed at compile time: the switch on kz
 // sits outside the loop, so a warp whose rays share a dominant axis runs one variant.
 template <int KZ>
-__device__ __forceinline__ void leaf_wt(const GTri* __restrict__ tris, int first, int cnt, F3 o, const WtRay& w,
-                                        float tMin, float& tBest, int& best) {
+__device__ __forceinline__ void leaf_wt(const GTri* __restrict__ tris, const int32_t* tie, int first, int cnt, F3 o,
+                                        const WtRay& w, float tMin, float& tBest, int& best) {
     for (int k = 0; k < cnt; ++k) {
         float tt;
-        if (wt_tri<KZ>(tris[first + k], o, w, tMin, tBest, tt) && replaces(tt, first + k, tBest, best)) {
+        if (wt_tri<KZ>(tris[first + k], o, w, tMin, tBest, tt) && replaces(tt, first + k, tBest, best, tie)) {
             tBest = tt;
             best = first + k;
         }
@@ -476,14 +484,14 @@ struct Walker<false> {
                 const int first = code >> 4, cnt = code & 15;
                 if constexpr (kWT) {
                     switch (wr.kz) {
-                        case 0: leaf_wt<0>(S.tris, first, cnt, o, wr, tMin, tBest, best); break;
-                        case 1: leaf_wt<1>(S.tris, first, cnt, o, wr, tMin, tBest, best); break;
-                        default: leaf_wt<2>(S.tris, first, cnt, o, wr, tMin, tBest, best); break;
+                        case 0: leaf_wt<0>(S.tris, S.tie, first, cnt, o, wr, tMin, tBest, best); break;
+                        case 1: leaf_wt<1>(S.tris, S.tie, first, cnt, o, wr, tMin, tBest, best); break;
+                        default: leaf_wt<2>(S.tris, S.tie, first, cnt, o, wr, tMin, tBest, best); break;
                     }
                 } else {
                     for (int k = 0; k < cnt; ++k) {
                         float tt;
-                        if (mt_f(S.tris[first + k], o, d, tMin, tBest, tt) && replaces(tt, first + k, tBest, best)) {
+                        if (mt_f(S.tris[first + k], o, d, tMin, tBest, tt) && replaces(tt, first + k, tBest, best, S.tie)) {
                             tBest = tt;
                             best = first + k;
                         }
@@ -588,9 +596,9 @@ struct Walker8 {
                 const int code = ~ref;
                 const int first = code >> 4, cnt = code & 15;
                 switch (wr.kz) {
-                    case 0: leaf_wt<0>(S.tris, first, cnt, o, wr, tMin, tBest, best); break;
-                    case 1: leaf_wt<1>(S.tris, first, cnt, o, wr, tMin, tBest, best); break;
-                    default: leaf_wt<2>(S.tris, first, cnt, o, wr, tMin, tBest, best); break;
+                    case 0: leaf_wt<0>(S.tris, S.tie, first, cnt, o, wr, tMin, tBest, best); break;
+                    case 1: leaf_wt<1>(S.tris, S.tie, first, cnt, o, wr, tMin, tBest, best); break;
+                    default: leaf_wt<2>(S.tris, S.tie, first, cnt, o, wr, tMin, tBest, best); break;
                 }
                 if (!pop()) return best;
             } while (ref < 0);
@@ -640,9 +648,9 @@ __device__ __forceinline__ int closest_speculative(const SceneView& S, F3 o, F3 
         const int code = ~leaf;
         const int first = code >> 4, cnt = code & 15;
         switch (wr.kz) {
-            case 0: leaf_wt<0>(S.tris, first, cnt, o, wr, tMin, tBest, best); break;
-            case 1: leaf_wt<1>(S.tris, first, cnt, o, wr, tMin, tBest, best); break;
-            default: leaf_wt<2>(S.tris, first, cnt, o, wr, tMin, tBest, best); break;
+            case 0: leaf_wt<0>(S.tris, S.tie, first, cnt, o, wr, tMin, tBest, best); break;
+            case 1: leaf_wt<1>(S.tris, S.tie, first, cnt, o, wr, tMin, tBest, best); break;
+            default: leaf_wt<2>(S.tris, S.tie, first, cnt, o, wr, tMin, tBest, best); break;
         }
     };
     for (;;) {
@@ -772,7 +780,7 @@ struct Walker<true> {
                 const int first = code >> 4, cnt = code & 15;
                 for (int k = 0; k < cnt; ++k) {
                     double tt;
-                    if (mt_d(S.tris64[first + k], o, d, tMin, tBest, tt) && replaces(tt, first + k, tBest, best)) {
+                    if (mt_d(S.tris64[first + k], o, d, tMin, tBest, tt) && replaces(tt, first + k, tBest, best, S.tie)) {
                         tBest = tt;
                         best = first + k;
                     }
