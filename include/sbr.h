@@ -88,7 +88,10 @@ typedef struct sbr_scene_info {
 /* Copies the indexed triangle mesh (xyz: nverts*3 floats, tri_idx: ntris*3
  * indices), builds the BVH (SAH tree on host threads, or on the GPU with
  * opts->gpu_build) and uploads it.  The caller keeps its buffers.  Replaces
- * rtRcsEntry.cu:115-196. */
+ * rtRcsEntry.cu:115-196.  A mesh that holds a triangle twice with opposite
+ * windings also gets each triangle's rank in the reference's closest-hit walk
+ * (one more host SAH build, 4 bytes per triangle on the device): on an exact tie
+ * the sweep keeps the triangle that walk keeps (src/cuda/rtKernels.cu:36). */
 sbr_status sbr_scene_create(const float* xyz, size_t nverts, const uint32_t* tri_idx, size_t ntris,
                             const sbr_build_opts* opts, sbr_scene** out);
 sbr_status sbr_scene_destroy(sbr_scene* scene);
