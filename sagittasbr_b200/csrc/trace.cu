@@ -529,7 +529,7 @@ __global__ void __launch_bounds__(128) k_trace_list(const TraceListParams P) {
 //                projected box first, then the three edges; each tile holds up to
 //                `cap` triangles and counts the rest;
 //   k_tile_hit   the closest hit of every ray of a tile among its list (the walk's
-//                test, nearest t then lowest slot), written to the first-hit buffer
+//                test, nearest t then the tie order), written to the first-hit buffer
 //                as a hit key, kZMiss, or kZWalk for a tile with more than `cap`
 //                triangles.
 // The trace reads each ray's first query from the buffer; every other query walks.

@@ -104,7 +104,7 @@ def test_hit_sequences(brute, name, prec):
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_first_hit_raster_matches_walk(golden, brute, name):
     """The first-hit tile raster (mixed precision) gives exactly the walk's records on
-    every ray (the closest hit is the nearest t, then the lowest slot, in both) and
+    every ray (the closest hit is the nearest t, then the tie order, in both) and
     bitwise the walk's fields, whether the tiles test their lists (cap 1024), walk
     (cap 1) or both (the default cap); FP32 plans asked for the raster walk."""
     v, t, th, ph, fr, nx, ny, G, mb, R = CASES[name]
